@@ -1,0 +1,331 @@
+"""Benchmark: FastScan top-1000 -> RankQuant b=2 rerank (k=10) over N=171,332
+dim-1024 docs -- the FastScan two-stage configuration -- on B200.
+
+One step = one batch of 1000 synthetic queries through the whole two-stage
+path.  Prints ONE JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value  : device-timed QPS of the batched form (all queries of a step in one
+         fused call), queries resident in HBM; L2 flushed (256 MiB write)
+         between steps, outside the timed region.
+e2e    : the same step through the public C ABI (ovb_two_stage_search) from
+         pinned host buffers: H2D of the queries and D2H of the top-10 inside
+         the timed region.
+plain  : one query per launch (device pointers), p50/p99 latency and QPS, and
+         whether its top-10 ids equal the batched form's.
+cpu_baseline / --impl reference: the CPU oracle's AVX-512 + OpenMP restatement
+         of the reference path (the Rust crate cannot be built here), all host
+         threads, on a bounded query sample.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "QPS & scan HBM GB/s vs peak, batched vs plain GPU @ identical top-10; p50/p99 ms"
+N_DOCS, DIM, NQ, K, M = 171_332, 1024, 1000, 10, 1000
+SEED = 0x0DD5EED2
+WORKLOAD = (f"fastscan_two_stage: RankQuantFastscan top-{M} -> RankQuant b=2 asymmetric rerank top-{K}; "
+            f"N={N_DOCS} dim={DIM}; {NQ} queries per step")
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_two_stage_qps(docs, queries, budget_s: float):
+    """Time the oracle's AVX-512/OpenMP restatement on a bounded query sample."""
+    from oracle import oracle as orc
+
+    blocks = orc.fastscan_pack(docs, DIM)
+    packed = orc.rankquant_encode(docs, DIM, 2)
+    threads = orc.max_threads()
+    probe = min(len(queries), max(threads, 8))
+    t0 = time.perf_counter()
+    orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[:probe], M, K, threads)
+    dt = time.perf_counter() - t0
+    sample = int(min(len(queries), max(probe, probe * budget_s / max(dt, 1e-6))))
+    t0 = time.perf_counter()
+    s, i = orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[:sample], M, K, threads)
+    dt = time.perf_counter() - t0
+    return sample / dt, threads, sample, (s, i), blocks, packed
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import ordvec_b200 as ob
+    from oracle import oracle as orc
+
+    docs = ob.synth_docs(SEED, N_DOCS, DIM)
+    queries, _ = ob.synth_queries(SEED, N_DOCS, NQ, DIM)
+    blocks = orc.fastscan_pack(docs, DIM)
+    packed = orc.rankquant_encode(docs, DIM, 2)
+    threads = orc.max_threads()
+    # size each step so the whole run stays within a few minutes
+    t0 = time.perf_counter()
+    orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[:threads], M, K, threads)
+    per_q = (time.perf_counter() - t0) / threads
+    per_step = int(max(threads, min(NQ, 20.0 / max(per_q, 1e-9) / max(args.steps + args.warmup, 1))))
+    for w in range(args.warmup):
+        orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[:per_step], M, K, threads)
+    t0 = time.perf_counter()
+    done = 0
+    for s in range(args.steps):
+        off = (s * per_step) % max(NQ - per_step + 1, 1)
+        orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[off:off + per_step], M, K, threads)
+        done += per_step
+    dt = time.perf_counter() - t0
+    qps = done / dt
+    line = {"impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8-lut/u32-acc/f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "queries_per_step_sampled": per_step},
+            "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
+                             "sample": f"{per_step} queries per step x {args.steps} steps"},
+            "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--plain-queries", type=int, default=200)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+
+    import ordvec_b200 as ob
+    from ordvec_b200._lib import check, lib
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ob.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    docs = ob.synth_docs(SEED, N_DOCS, DIM)
+    queries, planted = ob.synth_queries(SEED + 1000 * rank, N_DOCS, NQ, DIM)
+    rq = ob.RankQuant(DIM, 2)
+    rq.add(docs)
+    fs = ob.RankQuantFastscan(DIM)
+    fs.add(docs)
+
+    dev = torch.device("cuda", local)
+    d_q = torch.from_numpy(queries).to(dev)
+    d_s = torch.empty(NQ * K, dtype=torch.float32, device=dev)
+    d_i = torch.empty(NQ * K, dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def step_device(nq=NQ, q_ptr=None, s_ptr=None, i_ptr=None):
+        ob.two_stage_search_device(rq, fs, q_ptr or d_q.data_ptr(), nq, M, K, s_ptr or d_s.data_ptr(),
+                                   i_ptr or d_i.data_ptr(), sp)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step_device()
+    barrier()
+    launches_per_step = ob.last_launch_count()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    # ---- value: device-timed batched steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    for s in range(args.steps):
+        flush.fill_(s & 0xFF)
+        ev[s][0].record(stream)
+        step_device()
+        ev[s][1].record(stream)
+    barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = max_over_ranks(sum(step_ms))
+    batched_ids = d_i.view(NQ, K).cpu().numpy()
+
+    # ---- e2e: public C ABI, pinned host buffers, H2D + D2H inside the timed region
+    h_q = torch.from_numpy(queries).pin_memory()
+    h_s = torch.empty(NQ * K, dtype=torch.float32).pin_memory()
+    h_i = torch.empty(NQ * K, dtype=torch.int64).pin_memory()
+    e2e_ms = []
+    for s in range(args.warmup + args.steps):
+        flush.fill_(s & 0xFF)
+        barrier()
+        t0 = time.perf_counter()
+        check(lib().ovb_two_stage_search(rq.handle, fs.handle, C.c_void_p(h_q.data_ptr()), NQ, M, K,
+                                         C.c_void_p(h_s.data_ptr()), C.c_void_p(h_i.data_ptr())))
+        dt = (time.perf_counter() - t0) * 1e3
+        if s >= args.warmup:
+            e2e_ms.append(dt)
+    e2e_total = max_over_ranks(sum(e2e_ms))
+    e2e_same = bool(np.array_equal(h_i.numpy().reshape(NQ, K), batched_ids))
+
+    # ---- plain: one query per launch
+    P = min(args.plain_queries, NQ)
+    pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(P)]
+    p_s = torch.empty(P * K, dtype=torch.float32, device=dev)
+    p_i = torch.empty(P * K, dtype=torch.int64, device=dev)
+    for qi in range(3):
+        step_device(1, d_q[qi].data_ptr(), p_s[qi * K:].data_ptr(), p_i[qi * K:].data_ptr())
+    barrier()
+    for qi in range(P):
+        flush.fill_(qi & 0xFF)
+        pev[qi][0].record(stream)
+        step_device(1, d_q[qi].data_ptr(), p_s[qi * K:].data_ptr(), p_i[qi * K:].data_ptr())
+        pev[qi][1].record(stream)
+    barrier()
+    plain_ms = [a.elapsed_time(b) for a, b in pev]
+    plain_launches = ob.last_launch_count()
+    identical = bool(np.array_equal(p_i.view(P, K).cpu().numpy(), batched_ids[:P]))
+    clock_info = clocks.stop()
+
+    # ---- stage profile (roofline of the dominant kernel)
+    flush.fill_(1)
+    barrier()
+    stages = ob.two_stage_profile(rq, fs, d_q.data_ptr(), NQ, M, K, d_s.data_ptr(), d_i.data_ptr(), sp)
+    flush.fill_(2)
+    barrier()
+    stages1 = ob.two_stage_profile(rq, fs, d_q.data_ptr(), 1, M, K, d_s.data_ptr(), d_i.data_ptr(), sp)
+
+    peak, peak_kind = measured_peaks()
+    pairs_pad = ((DIM // 2 + 31) // 32) * 32
+    code_bytes = ((N_DOCS + 31) // 32) * 16 * pairs_pad  # device layout, read once per launch
+    ref_code_bytes = ((N_DOCS + 31) // 32) * (DIM // 2) * 32
+
+    def scan_bytes(nq):  # codes once + per-query LUTs + the key row written per query
+        return code_bytes + nq * pairs_pad * 16 + nq * N_DOCS * 4
+
+    def roof(nq, ms):
+        achieved = scan_bytes(nq) / (ms * 1e-3) / 1e9
+        return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "fastscan_scan_kernel", "queries_per_launch": nq,
+                "algorithmic_bytes_per_launch": scan_bytes(nq), "launch_ms": ms, "peak_source": peak_kind}
+
+    value = world * NQ * args.steps / (total_ms * 1e-3)
+    e2e = world * NQ * args.steps / (e2e_total * 1e-3)
+    plain_qps = 1e3 / statistics.mean(plain_ms)
+    line = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8-lut/u32-acc/f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_docs": N_DOCS, "dim": DIM, "queries_per_step_per_gpu": NQ, "k": K,
+                   "candidates": M, "form": "batched (one fused two-stage call per step)",
+                   "l2": "flushed between steps by a 256 MiB device write (outside the timed region)",
+                   "parallelism": f"replicas x{world} (queries sharded per rank, no data-path collective)"},
+        "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": NQ * DIM * 4,
+                "d2h_bytes_per_step": NQ * K * (4 + 8), "ms_per_step": e2e_total / args.steps,
+                "top10_equal_to_device_path": e2e_same},
+        "gpu_launches": launches_per_step * args.steps,
+        "plain": {"qps": plain_qps, "p50_ms": float(np.percentile(plain_ms, 50)),
+                  "p99_ms": float(np.percentile(plain_ms, 99)), "queries": P, "launches_per_query": plain_launches,
+                  "identical_top10_vs_batched": identical, "batched_over_plain": value / world / plain_qps},
+        "stages_ms": dict(zip(["prep", "scan", "select", "rerank", "final_select"], stages)),
+        "stages_ms_plain": dict(zip(["prep", "scan", "select", "rerank", "final_select"], stages1)),
+        "scan_gbs_effective": NQ * ref_code_bytes / (stages[1] * 1e-3) / 1e9,
+        "roofline": roof(NQ, stages[1]),
+        "roofline_plain": roof(1, stages1[1]),
+        "clocks": clock_info,
+    }
+    if rank == 0 and not args.no_cpu:
+        qps, threads, sample, _, _, _ = cpu_two_stage_qps(docs, queries, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
+                                "sample": f"first {sample} of the step's {NQ} queries, all host threads"}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,439 @@
+"""Python mirror of ordvec's scan-path API, backed by the B200 kernels.
+
+Class and method names, argument meaning, clamping and result shapes follow
+the reference crate (ordvec 0.6.0): ``RankQuant`` (src/quant.rs),
+``SignBitmap`` (src/sign_bitmap.rs), ``Bitmap`` (src/bitmap.rs),
+``RankQuantFastscan`` (src/fastscan.rs), ``MultiBucketBitmap``
+(src/multi_bucket.rs), ``TwoStageCandidatePolicy`` and ``SearchResults``
+(src/lib.rs:313-415).  Inputs and outputs are numpy arrays in host memory;
+codes live in HBM for the lifetime of the object.  Where the reference
+panics on a contract violation this raises ``OrdvecError`` (a ValueError).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from ._lib import (KIND_BITMAP, KIND_FASTSCAN, KIND_MULTIBUCKET, KIND_RANK_QUANT, KIND_SIGN_BITMAP,
+                   IndexInfo, OrdvecError, check, lib)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _rows(x, dim: int) -> np.ndarray:
+    a = np.ascontiguousarray(x, dtype=np.float32).reshape(-1)
+    if a.size % dim:
+        raise OrdvecError(2, f"queries length {a.size} must be a multiple of dim {dim}")
+    return a
+
+
+@dataclass
+class SearchResults:
+    """Flat nq*k scores and ids (src/lib.rs:313-415)."""
+
+    scores: np.ndarray
+    indices: np.ndarray
+    nq: int
+    k: int
+
+    def scores_for_query(self, qi: int) -> np.ndarray:
+        return self.scores[qi * self.k:(qi + 1) * self.k]
+
+    def indices_for_query(self, qi: int) -> np.ndarray:
+        return self.indices[qi * self.k:(qi + 1) * self.k]
+
+
+@dataclass
+class CandidateBatch:
+    """CSR candidate rows (src/sign_bitmap.rs:60-86)."""
+
+    candidates: np.ndarray
+    offsets: np.ndarray
+
+    def query_count(self) -> int:
+        return max(len(self.offsets) - 1, 0)
+
+    def candidates_for_query(self, qi: int) -> Optional[np.ndarray]:
+        if qi + 1 >= len(self.offsets):
+            return None
+        return self.candidates[self.offsets[qi]:self.offsets[qi + 1]]
+
+
+@dataclass(frozen=True)
+class TwoStageCandidatePolicy:
+    """src/quant.rs:234-262."""
+
+    min_candidates: int = 256
+    k_multiplier: int = 32
+    max_candidates: Optional[int] = None
+
+    def candidate_count(self, k: int, search_space: int) -> int:
+        if k == 0 or search_space == 0:
+            return 0
+        count = max(self.min_candidates, min(k * self.k_multiplier, 2**64 - 1))
+        if self.max_candidates is not None:
+            count = min(count, self.max_candidates)
+        return min(count, search_space)
+
+
+class _Index:
+    """Owns one device-resident index handle."""
+
+    _kind = 0
+
+    def __init__(self, handle):
+        self._h = handle
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().ordvec_index_free(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> IndexInfo:
+        info = IndexInfo()
+        lib().ordvec_index_info_init(C.byref(info))
+        check(lib().ordvec_index_info(self._h, C.byref(info)))
+        return info
+
+    def __len__(self) -> int:
+        return int(self.info().vector_count)
+
+    def len(self) -> int:
+        return len(self)
+
+    def is_empty(self) -> bool:
+        return len(self) == 0
+
+    @property
+    def dim(self) -> int:
+        return int(self.info().dim)
+
+    def bytes_per_vec(self) -> int:
+        return int(self.info().bytes_per_vec)
+
+    def add(self, vectors) -> None:
+        v = _rows(vectors, self.dim)
+        check(lib().ovb_index_add(self._h, _ptr(v), v.size // self.dim))
+
+    def add_device(self, device_ptr: int, n: int) -> None:
+        check(lib().ovb_index_add_device(self._h, C.c_void_p(device_ptr), n))
+
+    def write(self, path: str) -> None:
+        check(lib().ovb_index_write(self._h, str(path).encode()))
+
+    def payload(self) -> np.ndarray:
+        """Codes in the reference's persisted payload layout (bytes)."""
+        n = C.c_uint64()
+        check(lib().ovb_index_payload_bytes(self._h, C.byref(n)))
+        out = np.empty(max(n.value, 1), np.uint8)
+        check(lib().ovb_index_payload(self._h, _ptr(out), n.value))
+        return out[: n.value]
+
+    @classmethod
+    def _wrap_loaded(cls, handle):
+        obj = cls.__new__(cls)
+        _Index.__init__(obj, handle)
+        return obj
+
+
+def _new(fn, *args):
+    h = C.c_void_p()
+    check(fn(*args, C.byref(h)))
+    return h
+
+
+def load(path: str):
+    """Load any of .ovrq / .ovbm / .ovsb / .ovfs into HBM (src/rank_io.rs)."""
+    h = C.c_void_p()
+    check(lib().ovb_index_load_any(str(path).encode(), 0, C.byref(h)))
+    info = IndexInfo()
+    lib().ordvec_index_info_init(C.byref(info))
+    check(lib().ordvec_index_info(h, C.byref(info)))
+    cls = {KIND_RANK_QUANT: RankQuant, KIND_BITMAP: Bitmap, KIND_SIGN_BITMAP: SignBitmap,
+           KIND_FASTSCAN: RankQuantFastscan}[info.kind]
+    return cls._wrap_loaded(h)
+
+
+class RankQuant(_Index):
+    """B-bit bucketed-rank index (src/quant.rs:211-1509)."""
+
+    def __init__(self, dim: int, bits: int):
+        super().__init__(_new(lib().ovb_rankquant_new, dim, bits))
+
+    @property
+    def bits(self) -> int:
+        return int(self.info().bit_width)
+
+    @classmethod
+    def load(cls, path: str) -> "RankQuant":
+        obj = load(path)
+        if not isinstance(obj, RankQuant):
+            raise OrdvecError(4, "not a RankQuant index")
+        return obj
+
+    def search_asymmetric(self, queries, k: int) -> SearchResults:
+        """src/quant.rs:713-847: nq x min(k, n), (score desc, id asc)."""
+        dim = self.dim
+        q = _rows(queries, dim)
+        nq = q.size // dim
+        ke = min(k, len(self))
+        s = np.empty(max(nq * ke, 1), np.float32)
+        i = np.empty(max(nq * ke, 1), np.int64)
+        check(lib().ovb_rankquant_search(self._h, _ptr(q), nq, ke, _ptr(s), _ptr(i)))
+        if ke == 0:
+            return SearchResults(np.zeros(0, np.float32), np.full(0, -1, np.int64), nq, 0)
+        return SearchResults(s[: nq * ke], i[: nq * ke], nq, ke)
+
+    def search_asymmetric_subset_batched_serial(self, queries, candidate_offsets, candidates, k) -> SearchResults:
+        """src/quant.rs:1336-1451: rectangular nq x min(k, n), sentinel padded."""
+        dim = self.dim
+        q = _rows(queries, dim)
+        nq = q.size // dim
+        off = np.ascontiguousarray(candidate_offsets, np.uint64)
+        cand = np.ascontiguousarray(candidates, np.uint32)
+        if off.size != nq + 1:
+            raise OrdvecError(2, f"candidate_offsets length {off.size} must be nq+1 ({nq + 1})")
+        if off[-1] != cand.size:
+            raise OrdvecError(2, "candidate_offsets[nq] must equal candidates.len()")
+        out_k = min(k, len(self))
+        s = np.empty(max(nq * out_k, 1), np.float32)
+        i = np.empty(max(nq * out_k, 1), np.int64)
+        c = cand if cand.size else np.zeros(1, np.uint32)
+        check(lib().ovb_rankquant_search_subset(self._h, _ptr(q), nq, _ptr(off), _ptr(c), out_k, _ptr(s), _ptr(i)))
+        return SearchResults(s[: nq * out_k], i[: nq * out_k], nq, out_k)
+
+    def search_asymmetric_subset(self, query, candidates, k: int):
+        """src/quant.rs:1048-1083: returns (scores, ids) of length min(k, m)."""
+        cand = np.ascontiguousarray(candidates, np.uint32)
+        if cand.size > len(self):
+            raise OrdvecError(12, f"search_asymmetric_subset: candidate list length {cand.size} exceeds "
+                                  f"n_vectors {len(self)}; deduplicate repeated ids before calling")
+        out_k = min(k, cand.size)
+        if out_k == 0:
+            return np.zeros(0, np.float32), np.zeros(0, np.int64)
+        res = self.search_asymmetric_subset_batched_serial(query, [0, cand.size], cand, out_k)
+        return res.scores[:out_k].copy(), res.indices[:out_k].copy()
+
+    def try_search_with_sign_probe_with_policy(self, sign_probe: "SignBitmap", query, k: int,
+                                               policy: TwoStageCandidatePolicy):
+        """src/quant.rs:1467-1498."""
+        if sign_probe.dim != self.dim:
+            raise OrdvecError(2, f"sign_probe.dim: must match RankQuant dim {self.dim}")
+        if len(sign_probe) != len(self):
+            raise OrdvecError(2, f"sign_probe.len: must match RankQuant len {len(self)}")
+        q = _rows(query, self.dim)
+        if q.size != self.dim:
+            raise OrdvecError(2, f"query: length {q.size}, expected {self.dim}")
+        m = policy.candidate_count(k, len(self))
+        cands = sign_probe.top_m_candidates(q, m)
+        return self.search_asymmetric_subset(q, cands, k)
+
+    def try_search_with_sign_probe(self, sign_probe: "SignBitmap", query, k: int):
+        return self.try_search_with_sign_probe_with_policy(sign_probe, query, k, TwoStageCandidatePolicy())
+
+    search_with_sign_probe = try_search_with_sign_probe
+
+
+class SignBitmap(_Index):
+    """1-bit sign fingerprints, Hamming candidate generation (src/sign_bitmap.rs)."""
+
+    def __init__(self, dim: int):
+        super().__init__(_new(lib().ovb_sign_bitmap_new, dim))
+
+    def _top_m(self, queries, m: int) -> np.ndarray:
+        dim = self.dim
+        q = _rows(queries, dim)
+        nq = q.size // dim
+        me = min(m, len(self))
+        out = np.empty(max(nq * me, 1), np.uint32)
+        check(lib().ovb_sign_bitmap_top_m(self._h, _ptr(q), nq, me, _ptr(out)))
+        return out[: nq * me].reshape(nq, me)
+
+    def top_m_candidates(self, q, m: int) -> np.ndarray:
+        return self._top_m(q, m)[0] if np.size(q) else np.zeros(0, np.uint32)
+
+    def top_m_candidates_batched(self, queries, m: int) -> List[np.ndarray]:
+        return list(self._top_m(queries, m))
+
+    def top_m_candidates_batched_serial_csr(self, queries, m: int) -> CandidateBatch:
+        rows = self._top_m(queries, m)
+        nq, me = rows.shape
+        return CandidateBatch(rows.reshape(-1).copy(), np.arange(nq + 1, dtype=np.uint64) * me)
+
+    def score_all(self, q) -> np.ndarray:
+        qq = _rows(q, self.dim)
+        out = np.empty(max(len(self), 1), np.uint32)
+        check(lib().ovb_sign_bitmap_score_all(self._h, _ptr(qq), _ptr(out)))
+        return out[: len(self)]
+
+
+class Bitmap(_Index):
+    """Constant-weight top-n_top bitmaps, AND-overlap scoring (src/bitmap.rs)."""
+
+    def __init__(self, dim: int, n_top: int):
+        super().__init__(_new(lib().ovb_bitmap_new, dim, n_top))
+
+    @property
+    def n_top(self) -> int:
+        return int(self.info().n_top)
+
+    def search(self, queries, k: int) -> SearchResults:
+        dim = self.dim
+        q = _rows(queries, dim)
+        nq = q.size // dim
+        ke = min(k, len(self))
+        s = np.empty(max(nq * ke, 1), np.float32)
+        i = np.empty(max(nq * ke, 1), np.int64)
+        check(lib().ovb_bitmap_search(self._h, _ptr(q), nq, ke, _ptr(s), _ptr(i)))
+        return SearchResults(s[: nq * ke], i[: nq * ke], nq, ke)
+
+    def _top_m(self, queries, m: int) -> np.ndarray:
+        dim = self.dim
+        q = _rows(queries, dim)
+        nq = q.size // dim
+        me = min(m, len(self))
+        out = np.empty(max(nq * me, 1), np.uint32)
+        check(lib().ovb_bitmap_top_m(self._h, _ptr(q), nq, me, _ptr(out)))
+        return out[: nq * me].reshape(nq, me)
+
+    def top_m_candidates(self, q, m: int) -> np.ndarray:
+        return self._top_m(q, m)[0]
+
+    def top_m_candidates_batched(self, queries, m: int) -> List[np.ndarray]:
+        return list(self._top_m(queries, m))
+
+    def search_subset(self, query, doc_ids, k: int):
+        """src/bitmap.rs:470-494 through the C ABI subset search."""
+        from .abi import index_search
+
+        hits = index_search(self, query, k, candidates=doc_ids)
+        return (np.array([h[2] for h in hits], np.float32), np.array([h[0] for h in hits], np.int64))
+
+
+class RankQuantFastscan(_Index):
+    """FastScan b=2 nibble-LUT index (src/fastscan.rs:532-705)."""
+
+    def __init__(self, dim: int):
+        super().__init__(_new(lib().ovb_fastscan_new, dim))
+
+    def search(self, queries, k: int) -> SearchResults:
+        dim = self.dim
+        q = _rows(queries, dim)
+        nq = q.size // dim
+        ke = min(k, len(self))
+        s = np.empty(max(nq * ke, 1), np.float32)
+        i = np.empty(max(nq * ke, 1), np.int64)
+        check(lib().ovb_fastscan_search(self._h, _ptr(q), nq, ke, _ptr(s), _ptr(i)))
+        return SearchResults(s[: nq * ke], i[: nq * ke], nq, ke)
+
+
+class MultiBucketBitmap(_Index):
+    """2^bits bucket bitmaps per document (src/multi_bucket.rs:58-251)."""
+
+    def __init__(self, dim: int, bits: int):
+        super().__init__(_new(lib().ovb_multibucket_new, dim, bits))
+
+    @property
+    def bits(self) -> int:
+        return int(self.info().bit_width)
+
+    def _nb(self):
+        return 1 << self.bits
+
+    def diagonal_weights(self) -> np.ndarray:
+        nb = self._nb()
+        return np.eye(nb, dtype=np.float32).reshape(-1)
+
+    def outer_product_weights(self) -> np.ndarray:
+        nb = self._nb()
+        c = np.float32((nb - 1.0) / 2.0)
+        a = np.arange(nb, dtype=np.float32) - c
+        return (a[:, None] * a[None, :]).astype(np.float32).reshape(-1)
+
+    def banded_weights(self, half_width: int) -> np.ndarray:
+        nb = self._nb()
+        w = self.outer_product_weights().reshape(nb, nb)
+        idx = np.arange(nb)
+        w[np.abs(idx[:, None] - idx[None, :]) > half_width] = 0.0
+        return w.reshape(-1)
+
+    def top_m_bilinear_batched(self, queries, weights, m: int) -> np.ndarray:
+        """Query bitmaps from ranks (src/multi_bucket.rs:122-137), then the
+        bilinear top-m (src/multi_bucket.rs:228-251), order (score desc, id asc)."""
+        dim = self.dim
+        q = _rows(queries, dim)
+        nq = q.size // dim
+        w = np.ascontiguousarray(weights, np.float32)
+        if w.size != self._nb() ** 2:
+            raise OrdvecError(2, "weights must be nb x nb")
+        me = min(m, len(self))
+        out = np.empty(max(nq * me, 1), np.uint32)
+        check(lib().ovb_multibucket_top_m(self._h, _ptr(q), nq, _ptr(w), me, _ptr(out)))
+        return out[: nq * me].reshape(nq, me)
+
+
+def two_stage_search(rq: RankQuant, stage1: _Index, queries, m: int, k: int) -> SearchResults:
+    """Fused candidate generation (sign / FastScan / Bitmap / multi-bucket) and
+    RankQuant rerank on the device; m = 0 uses TwoStageCandidatePolicy()."""
+    dim = rq.dim
+    q = _rows(queries, dim)
+    nq = q.size // dim
+    me = m if m else TwoStageCandidatePolicy().candidate_count(k, len(rq))
+    me = min(me, len(rq))
+    ke = min(k, me)
+    s = np.empty(max(nq * ke, 1), np.float32)
+    i = np.empty(max(nq * ke, 1), np.int64)
+    check(lib().ovb_two_stage_search(rq.handle, stage1.handle, _ptr(q), nq, m, k, _ptr(s), _ptr(i)))
+    return SearchResults(s[: nq * ke], i[: nq * ke], nq, ke)
+
+
+def synth_docs(seed: int, n: int, dim: int, sigma: float = 0.3, first: int = 0) -> np.ndarray:
+    out = np.empty((n, dim), np.float32)
+    check(lib().ovb_synth_docs(seed, first, n, dim, sigma, _ptr(out)))
+    return out
+
+
+def synth_queries(seed: int, n_docs: int, nq: int, dim: int, doc_sigma: float = 0.3,
+                  query_sigma: float = 0.1):
+    out = np.empty((nq, dim), np.float32)
+    planted = np.empty(nq, np.uint64)
+    check(lib().ovb_synth_queries(seed, n_docs, nq, dim, doc_sigma, query_sigma, _ptr(out), _ptr(planted)))
+    return out, planted
+
+
+def last_launch_count() -> int:
+    return int(lib().ovb_last_launch_count())
+
+
+def set_device(device: int) -> None:
+    check(lib().ovb_set_device(device))
+
+
+def two_stage_search_device(rq: RankQuant, stage1: _Index, d_queries: int, nq: int, m: int, k: int,
+                            d_scores: int, d_ids: int, stream: int) -> None:
+    """Device-pointer two-stage search, asynchronous on `stream` (cudaStream_t as int)."""
+    check(lib().ovb_two_stage_search_device(rq.handle, stage1.handle, C.c_void_p(d_queries), nq, m, k,
+                                            C.c_void_p(d_scores), C.c_void_p(d_ids), C.c_void_p(stream)))
+
+
+def two_stage_profile(rq: RankQuant, stage1: _Index, d_queries: int, nq: int, m: int, k: int,
+                      d_scores: int, d_ids: int, stream: int) -> List[float]:
+    """Synchronous device-pointer two-stage search returning per-stage device ms:
+    [prep, stage-1 scan, stage-1 select, rerank scoring, final select]."""
+    ms = (C.c_float * 5)()
+    check(lib().ovb_two_stage_profile(rq.handle, stage1.handle, C.c_void_p(d_queries), nq, m, k,
+                                      C.c_void_p(d_scores), C.c_void_p(d_ids), C.c_void_p(stream), ms))
+    return list(ms)

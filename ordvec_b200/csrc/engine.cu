@@ -1,0 +1,231 @@
+// Device pipelines: scan -> key matrix -> exact top-k select, and the fused
+// two-stage (candidate generation -> asymmetric rerank) flow.
+//
+// Each pipeline takes device query rows and leaves its result in the calling
+// thread's workspace (out_keys / out_ids, rows of k_eff entries, sentinel
+// padded).  Queries are processed in chunks so the key matrix (nq_chunk x n
+// u32) stays within a fixed HBM budget (OVB_KEYS_BUDGET_MB, default 2048).
+#include <cmath>
+#include <cstdlib>
+
+#include "ovb_host.h"
+
+namespace ovb {
+
+namespace {
+
+uint64_t keys_budget() {
+  static const uint64_t b = [] {
+    const char* e = getenv("OVB_KEYS_BUDGET_MB");
+    uint64_t mb = e ? strtoull(e, nullptr, 10) : 2048;
+    return (mb ? mb : 2048) << 20;
+  }();
+  return b;
+}
+
+// rankquant_norm (src/rank.rs:275-280) and 1/norm in f32, as the reference.
+float inv_rankquant_norm(uint32_t dim, uint32_t bits) {
+  const double n = (double)(1u << bits);
+  const float norm = (float)std::sqrt((double)dim * ((n * n - 1.0) / 12.0));
+  return 1.0f / norm;
+}
+
+void select_rows(Workspace& w, const uint32_t* keys, const uint32_t* ids, const uint64_t* row_off,
+                 uint64_t ld, uint64_t n, uint64_t rows, uint32_t k, uint32_t key_bits,
+                 uint32_t id_bits, uint32_t* out_keys, uint32_t* out_ids, cudaStream_t st) {
+  SelectArgs a{keys, ids, row_off, ld, n, k, key_bits, id_bits, out_keys, out_ids};
+  size_t se = select_rows_scratch_elems(rows, k);
+  uint64_t* scratch = se ? (uint64_t*)w.scratch.ensure(se * 8) : nullptr;
+  launch_select_rows(a, rows, scratch, st);
+}
+
+// scan(q0, qn, keys) writes keys[qn][n]; rows are selected into out[nq][k].
+template <class F>
+void full_scan_select(Workspace& w, uint64_t nq, uint64_t n, uint32_t k, uint32_t key_bits,
+                      uint32_t* out_keys, uint32_t* out_ids, cudaStream_t st, F&& scan) {
+  const uint64_t per_q = n * 4;
+  uint64_t qc = keys_budget() / per_q;
+  if (qc < 1) qc = 1;
+  if (qc > nq) qc = nq;
+  uint32_t* keys = (uint32_t*)w.keys.ensure(qc * per_q);
+  const uint32_t id_bits = bits_for(n - 1);
+  for (uint64_t q0 = 0; q0 < nq; q0 += qc) {
+    const uint64_t qn = nq - q0 < qc ? nq - q0 : qc;
+    scan(q0, qn, keys);
+    w.mark(st, 2);
+    select_rows(w, keys, nullptr, nullptr, n, n, qn, k, key_bits, id_bits, out_keys + q0 * k,
+                out_ids + q0 * k, st);
+    w.mark(st, 3);
+  }
+}
+
+float* normalised(Workspace& w, const float* d_q, uint64_t nq, uint32_t dim, cudaStream_t st) {
+  float* qu = (float*)w.q_unit.ensure(nq * dim * 4);
+  launch_l2_normalise(d_q, nq, dim, qu, st);
+  return qu;
+}
+
+void require_kind(const Index& ix, uint32_t kind, const char* what) {
+  if (ix.kind != kind) fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, std::string(what) + ": wrong index kind");
+}
+
+}  // namespace
+
+uint64_t default_candidate_count(uint64_t k, uint64_t space) {
+  // TwoStageCandidatePolicy::default() (src/quant.rs:242-262): min 256, k*32.
+  if (k == 0 || space == 0) return 0;
+  uint64_t prod = k > UINT64_MAX / 32 ? UINT64_MAX : k * 32;
+  uint64_t c = prod > 256 ? prod : 256;
+  return c < space ? c : space;
+}
+
+uint32_t engine_rankquant_full(const Index& rq, const float* d_q, uint64_t nq, uint64_t k,
+                               Workspace& w, cudaStream_t st) {
+  require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "search_asymmetric");
+  const uint32_t ke = (uint32_t)(k < rq.n ? k : rq.n);
+  if (!ke || !nq) return ke;
+  const float* qu = normalised(w, d_q, nq, rq.dim, st);
+  const float inv_norm = inv_rankquant_norm(rq.dim, rq.bits);
+  uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
+  uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
+  full_scan_select(w, nq, rq.n, ke, 32, ok, oi, st, [&](uint64_t q0, uint64_t qn, uint32_t* keys) {
+    launch_asym_scan(rq.codes.as<uint8_t>(), rq.n, rq.dim, rq.bits, qu + q0 * rq.dim, qn, inv_norm, keys,
+                     rq.n, st);
+  });
+  return ke;
+}
+
+uint32_t engine_rankquant_subset(const Index& rq, const float* d_q, uint64_t nq,
+                                 const uint64_t* d_off, const uint32_t* d_cands, uint64_t max_row,
+                                 uint64_t k, Workspace& w, cudaStream_t st) {
+  require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "search_asymmetric_subset");
+  const uint32_t ke = (uint32_t)(k < rq.n ? k : rq.n);
+  if (!ke || !nq) return ke;
+  const float* qu = normalised(w, d_q, nq, rq.dim, st);
+  const float inv_norm = inv_rankquant_norm(rq.dim, rq.bits);
+  // total entries = d_off[nq]; the caller sized keys2 through max_row * nq
+  uint32_t* keys = (uint32_t*)w.keys2.ensure((max_row ? max_row : 1) * nq * 4);
+  launch_asym_subset(rq.codes.as<uint8_t>(), rq.dim, rq.bits, qu, nq, d_off, d_cands, max_row, inv_norm,
+                     keys, st);
+  uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
+  uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
+  select_rows(w, keys, d_cands, d_off, 0, 0, nq, ke, 32, bits_for(rq.n - 1), ok, oi, st);
+  return ke;
+}
+
+// Stage-1 candidates into w.sel_keys / w.sel_ids, rows of m_eff ids.
+uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint64_t m,
+                           const float* d_weights, Workspace& w, cudaStream_t st) {
+  const uint32_t me = (uint32_t)(m < s1.n ? m : s1.n);
+  if (!me || !nq) return me;
+  uint32_t* sk = (uint32_t*)w.sel_keys.ensure(nq * me * 4);
+  uint32_t* si = (uint32_t*)w.sel_ids.ensure(nq * me * 4);
+  const uint64_t n = s1.n;
+  switch (s1.kind) {
+    case OVB_INDEX_KIND_SIGN_BITMAP:
+    case ORDVEC_INDEX_KIND_BITMAP: {
+      const int mode = s1.kind == OVB_INDEX_KIND_SIGN_BITMAP ? 0 : 1;
+      uint64_t* qb = (uint64_t*)w.qbits.ensure(nq * s1.qpv() * 8);
+      if (mode == 0)
+        launch_sign_query(d_q, nq, s1.dim, qb, st);
+      else
+        launch_bitmap_query(d_q, nq, s1.dim, s1.n_top, qb, st);
+      w.mark(st, 1);
+      const uint32_t key_bits = bits_for(mode == 0 ? s1.dim : s1.n_top);
+      full_scan_select(w, nq, n, me, key_bits, sk, si, st, [&](uint64_t q0, uint64_t qn, uint32_t* keys) {
+        launch_popc_scan(mode, s1.codes.as<uint64_t>(), n, s1.qpv(), qb + q0 * s1.qpv(), qn, s1.n_top, keys,
+                         n, st);
+      });
+      break;
+    }
+    case OVB_INDEX_KIND_FASTSCAN: {
+      const float* qu = normalised(w, d_q, nq, s1.dim, st);
+      uint8_t* lut = (uint8_t*)w.lut.ensure(nq * s1.pairs_pad * 16);
+      float* bias = (float*)w.bias.ensure(nq * 4);
+      float* invq = (float*)w.invq.ensure(nq * 4);
+      launch_fastscan_lut(qu, nq, s1.dim, s1.pairs_pad, lut, bias, invq, st);
+      w.mark(st, 1);
+      const float inv_norm = inv_rankquant_norm(s1.dim, 2);
+      full_scan_select(w, nq, n, me, 32, sk, si, st, [&](uint64_t q0, uint64_t qn, uint32_t* keys) {
+        launch_fastscan_scan(s1.codes.as<uint8_t>(), n, s1.pairs_pad, lut + q0 * s1.pairs_pad * 16, bias + q0,
+                             invq + q0, inv_norm, qn, keys, n, st);
+      });
+      break;
+    }
+    case OVB_INDEX_KIND_MULTIBUCKET: {
+      const uint32_t nb = s1.nb(), qpb = s1.dim / 64;
+      uint64_t* qb = (uint64_t*)w.qbits.ensure(nq * nb * qpb * 8);
+      launch_multibucket_query(d_q, nq, s1.dim, s1.bits, qb, st);
+      w.mark(st, 1);
+      const float* wts = d_weights;
+      if (!wts) {  // diagonal weights (src/multi_bucket.rs:157-164)
+        std::vector<float> diag(nb * nb, 0.0f);
+        for (uint32_t a = 0; a < nb; a++) diag[a * nb + a] = 1.0f;
+        float* dw = (float*)w.weights.ensure(nb * nb * 4);
+        OVB_CUDA(cudaMemcpyAsync(dw, diag.data(), nb * nb * 4, cudaMemcpyHostToDevice, st));
+        OVB_CUDA(cudaStreamSynchronize(st));
+        wts = dw;
+      }
+      full_scan_select(w, nq, n, me, 32, sk, si, st, [&](uint64_t q0, uint64_t qn, uint32_t* keys) {
+        launch_multibucket_scan(s1.codes.as<uint64_t>(), n, qpb, nb, qb + q0 * nb * qpb, wts, qn, keys, n, st);
+      });
+      break;
+    }
+    default:
+      fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "index kind cannot generate candidates");
+  }
+  return me;
+}
+
+uint32_t engine_bitmap_full(const Index& bm, const float* d_q, uint64_t nq, uint64_t k,
+                            Workspace& w, cudaStream_t st) {
+  require_kind(bm, ORDVEC_INDEX_KIND_BITMAP, "Bitmap::search");
+  const uint32_t ke = engine_candidates(bm, d_q, nq, k, nullptr, w, st);
+  if (ke && nq) {
+    OVB_CUDA(cudaMemcpyAsync(w.out_keys.ensure(nq * ke * 4), w.sel_keys.p, nq * ke * 4,
+                             cudaMemcpyDeviceToDevice, st));
+    OVB_CUDA(cudaMemcpyAsync(w.out_ids.ensure(nq * ke * 4), w.sel_ids.p, nq * ke * 4,
+                             cudaMemcpyDeviceToDevice, st));
+  }
+  return ke;
+}
+
+uint32_t engine_fastscan_full(const Index& fs, const float* d_q, uint64_t nq, uint64_t k,
+                              Workspace& w, cudaStream_t st) {
+  require_kind(fs, OVB_INDEX_KIND_FASTSCAN, "RankQuantFastscan::search");
+  const uint32_t ke = engine_candidates(fs, d_q, nq, k, nullptr, w, st);
+  if (ke && nq) {
+    OVB_CUDA(cudaMemcpyAsync(w.out_keys.ensure(nq * ke * 4), w.sel_keys.p, nq * ke * 4,
+                             cudaMemcpyDeviceToDevice, st));
+    OVB_CUDA(cudaMemcpyAsync(w.out_ids.ensure(nq * ke * 4), w.sel_ids.p, nq * ke * 4,
+                             cudaMemcpyDeviceToDevice, st));
+  }
+  return ke;
+}
+
+uint32_t engine_two_stage(const Index& rq, const Index& s1, const float* d_q, uint64_t nq,
+                          uint64_t m, uint64_t k, Workspace& w, cudaStream_t st) {
+  require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "two-stage rerank");
+  if (s1.dim != rq.dim) fail(ORDVEC_STATUS_DIM_MISMATCH, "stage-1 index dim must match RankQuant dim");
+  if (s1.n != rq.n) fail(ORDVEC_STATUS_BAD_ARGUMENT, "stage-1 index len must match RankQuant len");
+  const uint64_t m_req = m ? m : default_candidate_count(k, rq.n);
+  w.mark(st, 0);
+  const uint32_t me = engine_candidates(s1, d_q, nq, m_req, nullptr, w, st);
+  const uint32_t ke = (uint32_t)(k < me ? k : me);
+  if (!ke || !nq) return ke;
+  uint64_t* off = (uint64_t*)w.off.ensure((nq + 1) * 8);
+  launch_uniform_offsets(off, nq, me, st);
+  const float* qu = normalised(w, d_q, nq, rq.dim, st);
+  const float inv_norm = inv_rankquant_norm(rq.dim, rq.bits);
+  uint32_t* keys = (uint32_t*)w.keys2.ensure(nq * me * 4);
+  launch_asym_subset(rq.codes.as<uint8_t>(), rq.dim, rq.bits, qu, nq, off, w.sel_ids.as<uint32_t>(), me,
+                     inv_norm, keys, st);
+  w.mark(st, 4);
+  uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
+  uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
+  select_rows(w, keys, w.sel_ids.as<uint32_t>(), off, 0, 0, nq, ke, 32, bits_for(rq.n - 1), ok, oi, st);
+  w.mark(st, 5);
+  return ke;
+}
+
+}  // namespace ovb

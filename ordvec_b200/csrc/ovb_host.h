@@ -1,0 +1,140 @@
+// Internal host-side types of libordvec_b200: index handles, device buffers,
+// per-thread workspaces and the status-carrying exception used at the C ABI.
+#pragma once
+#include <stdint.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/ordvec_b200.h"
+#include "ovb_common.cuh"
+#include "ovb_kernels.h"
+
+namespace ovb {
+
+struct ApiError {
+  ordvec_status_t status;
+  std::string msg;
+};
+[[noreturn]] inline void fail(ordvec_status_t s, std::string m) { throw ApiError{s, std::move(m)}; }
+
+// Grow-only device allocation.
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  void* ensure(size_t bytes) {
+    if (bytes > cap) {
+      if (p) cudaFree(p);
+      p = nullptr;
+      cap = 0;
+      OVB_CUDA(cudaMalloc(&p, bytes));
+      cap = bytes;
+    }
+    return p;
+  }
+  template <class T>
+  T* as() const {
+    return (T*)p;
+  }
+};
+
+// Grow-only pinned host allocation.
+struct HostBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  HostBuf() = default;
+  HostBuf(const HostBuf&) = delete;
+  HostBuf& operator=(const HostBuf&) = delete;
+  ~HostBuf() {
+    if (p) cudaFreeHost(p);
+  }
+  void* ensure(size_t bytes) {
+    if (bytes > cap) {
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+      cap = 0;
+      OVB_CUDA(cudaMallocHost(&p, bytes));
+      cap = bytes;
+    }
+    return p;
+  }
+};
+
+constexpr uint64_t kIndexMagic = 0x5849303032424F56ull;
+constexpr uint64_t kMaxVectors = 64ull * 1024 * 1024;  // src/rank_io.rs:136
+constexpr uint32_t kMaxDim = 65535;                     // src/rank_io.rs:119
+constexpr uint64_t kMaxSignDim = 1ull << 24;            // src/rank_io.rs:126
+constexpr uint32_t kMaxDeviceRankDim = 16384;           // device rank transform limit
+
+struct Index {
+  uint64_t magic = kIndexMagic;
+  uint32_t kind = 0, dim = 0, bits = 0, n_top = 0, pairs_pad = 0;
+  uint64_t n = 0;
+  uint64_t file_size = 0;
+  int device = 0;
+  DevBuf codes;
+
+  uint32_t qpv() const { return dim / 64; }
+  uint32_t nb() const { return 1u << bits; }
+  uint64_t bpv() const { return (uint64_t)dim * bits / 8; }
+  // bytes_per_vec as the reference reports it
+  uint64_t ref_bytes_per_vec() const;
+  // device bytes holding n rows
+  uint64_t device_bytes(uint64_t rows) const;
+};
+
+// Per-thread device scratch and stream.
+struct Workspace {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf q_raw, q_unit, qbits, lut, bias, invq, keys, sel_keys, sel_ids, off, keys2, out_keys,
+      out_ids, scores, ids, scratch, stage, weights, flag;
+  HostBuf pinned;
+  // stage markers for ovb_two_stage_profile (recorded only while prof is set)
+  cudaEvent_t prof_ev[6] = {};
+  bool prof = false;
+  void mark(cudaStream_t st, int i) {
+    if (prof) OVB_CUDA(cudaEventRecord(prof_ev[i], st));
+  }
+  Workspace();
+  ~Workspace();
+};
+
+Workspace& workspace();
+const Index& as_index(const ordvec_index_t* h);
+Index& as_index_mut(ordvec_index_t* h);
+void ensure_device();
+
+// pipelines on device pointers (engine.cpp); return the effective k
+uint32_t engine_rankquant_full(const Index& rq, const float* d_q, uint64_t nq, uint64_t k,
+                               Workspace& w, cudaStream_t st);
+uint32_t engine_rankquant_subset(const Index& rq, const float* d_q, uint64_t nq,
+                                 const uint64_t* d_off, const uint32_t* d_cands, uint64_t max_row,
+                                 uint64_t k, Workspace& w, cudaStream_t st);
+uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint64_t m,
+                           const float* d_weights, Workspace& w, cudaStream_t st);
+uint32_t engine_bitmap_full(const Index& bm, const float* d_q, uint64_t nq, uint64_t k,
+                            Workspace& w, cudaStream_t st);
+uint32_t engine_fastscan_full(const Index& fs, const float* d_q, uint64_t nq, uint64_t k,
+                              Workspace& w, cudaStream_t st);
+uint32_t engine_two_stage(const Index& rq, const Index& s1, const float* d_q, uint64_t nq,
+                          uint64_t m, uint64_t k, Workspace& w, cudaStream_t st);
+uint64_t default_candidate_count(uint64_t k, uint64_t space);
+
+// persistence (persist.cpp)
+std::unique_ptr<Index> load_index_file(const char* path, bool v1_only);
+void probe_index_file(const char* path, ordvec_index_info_t* info);
+void write_index_file(const Index& ix, const char* path);
+void read_payload(const Index& ix, std::vector<uint8_t>& out);
+void upload_payload(Index& ix, const uint8_t* payload, uint64_t bytes);
+
+extern thread_local uint64_t tl_last_launches;
+
+}  // namespace ovb

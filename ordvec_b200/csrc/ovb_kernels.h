@@ -1,0 +1,91 @@
+// Host-side launch interface of the sm_100a kernels.  All pointers are
+// device pointers; every launch is asynchronous on `stream`.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstddef>
+
+namespace ovb {
+
+// ---- K7 select (select.cu) ---------------------------------------------------
+constexpr uint32_t kSelectSmemCap = 4096;  // k up to this sorts in shared memory
+
+struct SelectArgs {
+  const uint32_t* keys;     // row r at keys + r*ld (or + row_off[r])
+  const uint32_t* ids;      // explicit global ids (same layout) or null = position
+  const uint64_t* row_off;  // ragged rows (rows+1 offsets) or null = uniform n
+  uint64_t ld;
+  uint64_t n;
+  uint32_t k;         // output stride; each row keeps min(k, n_row), rest sentinel
+  uint32_t key_bits;  // significant bits of key32
+  uint32_t id_bits;   // significant bits of id32
+  uint32_t* out_keys;
+  uint32_t* out_ids;
+};
+size_t select_rows_scratch_elems(uint64_t rows, uint32_t k);
+void launch_select_rows(const SelectArgs& a, uint64_t rows, uint64_t* scratch,
+                        cudaStream_t stream);
+
+// ---- K8 query preparation (prep.cu) ------------------------------------------
+void launch_l2_normalise(const float* q, uint64_t nq, uint32_t dim, float* out,
+                         cudaStream_t stream);
+void launch_sign_query(const float* q, uint64_t nq, uint32_t dim, uint64_t* out,
+                       cudaStream_t stream);
+void launch_bitmap_query(const float* q, uint64_t nq, uint32_t dim, uint32_t n_top,
+                         uint64_t* out, cudaStream_t stream);
+void launch_fastscan_lut(const float* q_unit, uint64_t nq, uint32_t dim, uint32_t pairs_pad,
+                         uint8_t* lut, float* bias_sum, float* inv_q, cudaStream_t stream);
+
+// ---- K1/K2/K6 popcount scans (scan_popc.cu) -> key32 [nq][ld] ------------------
+// mode 0: sign Hamming (key = hamming); mode 1: bitmap AND overlap
+// (key = n_top - overlap).
+void launch_popc_scan(int mode, const uint64_t* words, uint64_t n, uint32_t qpv,
+                      const uint64_t* qbits, uint64_t nq, uint32_t n_top, uint32_t* keys,
+                      uint64_t ld, cudaStream_t stream);
+// Subset form: key32 for CSR candidate entries (keys share the CSR layout).
+void launch_popc_subset(int mode, const uint64_t* words, uint32_t qpv, const uint64_t* qbits,
+                        uint64_t nq, const uint64_t* offsets, const uint32_t* cands,
+                        uint64_t max_row, uint32_t n_top, uint32_t* keys, cudaStream_t stream);
+// Multi-bucket bilinear score (desc float key).
+void launch_multibucket_scan(const uint64_t* words, uint64_t n, uint32_t qpb, uint32_t nb,
+                             const uint64_t* qbits, const float* w, uint64_t nq,
+                             uint32_t* keys, uint64_t ld, cudaStream_t stream);
+void launch_multibucket_query(const float* q, uint64_t nq, uint32_t dim, uint32_t bits,
+                              uint64_t* out, cudaStream_t stream);
+
+// ---- K3 FastScan (scan_fastscan.cu) --------------------------------------------
+void launch_fastscan_scan(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad,
+                          const uint8_t* lut, const float* bias_sum, const float* inv_q,
+                          float inv_norm, uint64_t nq, uint32_t* keys, uint64_t ld,
+                          cudaStream_t stream);
+void launch_fastscan_relayout(const uint8_t* ref_blocks, uint64_t n, uint32_t pairs,
+                              uint32_t pairs_pad, uint8_t* dev_blocks, cudaStream_t stream);
+
+// ---- K4/K5 asymmetric RankQuant scoring (scan_asym.cu) ---------------------------
+void launch_asym_scan(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_t bits,
+                      const float* q_unit, uint64_t nq, float inv_norm, uint32_t* keys,
+                      uint64_t ld, cudaStream_t stream);
+void launch_asym_subset(const uint8_t* codes, uint32_t dim, uint32_t bits, const float* q_unit,
+                        uint64_t nq, const uint64_t* offsets, const uint32_t* cands,
+                        uint64_t max_row, float inv_norm, uint32_t* keys, cudaStream_t stream);
+
+// ---- encoders (encode.cu) ----------------------------------------------------------
+// kind: 0 RankQuant packed codes, 1 sign bitmap, 2 const-weight bitmap, 3 FastScan
+// (device layout), 4 multi-bucket bitmaps.
+void launch_encode(int kind, const float* vecs, uint64_t n, uint32_t dim, uint32_t bits,
+                   uint32_t n_top, uint32_t pairs_pad, void* out, uint64_t first_doc,
+                   cudaStream_t stream);
+uint32_t fastscan_pairs_pad(uint32_t dim);
+uint64_t fastscan_block_bytes(uint32_t pairs_pad);
+
+// sets *flag (device u32, caller-zeroed) if any value is non-finite
+void launch_finite_flag(const float* x, uint64_t count, uint32_t* flag, cudaStream_t stream);
+
+// helper: key32 -> float score / sentinel mapping and uniform offsets
+void launch_uniform_offsets(uint64_t* off, uint64_t nq, uint64_t m, cudaStream_t stream);
+void launch_keys_to_results(const uint32_t* keys, const uint32_t* ids, uint64_t count,
+                            int mode, uint32_t n_top, float* scores, int64_t* out_ids,
+                            cudaStream_t stream);
+
+}  // namespace ovb

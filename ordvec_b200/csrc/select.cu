@@ -1,0 +1,206 @@
+// K7: exact, deterministic per-row top-k selection.
+//
+// Reproduces the reference's composite-key selection contract -- TopK
+// (src/util.rs:375-600), select_nth_unstable_by + head sort on
+// (score, doc_id) (src/sign_bitmap.rs:350-361, src/bitmap.rs:281-289) and the
+// ABI's normalize_global_order (ordvec-ffi/src/lib.rs:430-435) -- as a radix
+// select over the logical 64-bit key (key32 << 32) | id32, smaller is better.
+// Keys with equal (score, id) (duplicate candidate rows) are interchangeable:
+// any `need` of them give identical output, so no slot order is required.
+//
+// One CTA per row.  Per digit (11 bits at a time, most significant first,
+// skipping bits that are zero in every key) the CTA histograms the keys that
+// still match the fixed prefix, finds the bin holding the k-th key, and stops
+// as soon as that bin holds exactly the keys still needed.  A collect pass
+// then gathers the k winners and a bitonic sort orders them.
+#include "ovb_common.cuh"
+#include "ovb_kernels.h"
+
+namespace ovb {
+
+namespace {
+
+constexpr int kSelThreads = 1024;
+constexpr int kHistBins = 2048;
+
+struct Digit {
+  uint32_t shift, width;
+};
+
+__device__ __forceinline__ uint64_t load_key(const uint32_t* keys, const uint32_t* ids,
+                                             uint64_t i) {
+  uint32_t k = keys[i];
+  uint32_t id = ids ? ids[i] : (uint32_t)i;
+  return ((uint64_t)k << 32) | id;
+}
+
+// In-place bitonic sort of buf[0..len) ascending, len a power of two.
+__device__ void bitonic_sort(uint64_t* buf, uint32_t len) {
+  for (uint32_t size = 2; size <= len; size <<= 1) {
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      for (uint32_t t = threadIdx.x; t < len / 2; t += blockDim.x) {
+        uint32_t i = 2 * t - (t & (stride - 1));
+        uint32_t j = i + stride;
+        bool up = (i & size) == 0;
+        uint64_t a = buf[i], b = buf[j];
+        if ((a > b) == up) {
+          buf[i] = b;
+          buf[j] = a;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kSelThreads)
+    select_rows_kernel(SelectArgs a, uint64_t* gbuf, uint32_t gbuf_stride) {
+  __shared__ uint32_t hist[kHistBins];
+  __shared__ uint32_t warp_tot[kSelThreads / 32];
+  __shared__ uint64_t sbuf[kSelectSmemCap];
+  __shared__ uint32_t s_bin, s_before, s_in_bin, s_cnt_below, s_cnt_tie;
+
+  const uint64_t row = blockIdx.x;
+  uint64_t start, n;
+  if (a.row_off) {
+    start = a.row_off[row];
+    n = a.row_off[row + 1] - start;
+  } else {
+    start = row * a.ld;
+    n = a.n;
+  }
+  const uint32_t* keys = a.keys + start;
+  const uint32_t* ids = a.ids ? a.ids + start : nullptr;
+  const uint32_t k_eff = (uint32_t)(n < a.k ? n : a.k);
+  uint32_t* out_k = a.out_keys + row * (uint64_t)a.k;
+  uint32_t* out_i = a.out_ids + row * (uint64_t)a.k;
+
+  for (uint32_t j = k_eff + threadIdx.x; j < a.k; j += blockDim.x) {
+    out_k[j] = kSentinelKey;
+    out_i[j] = kSentinelId;
+  }
+  if (k_eff == 0) return;
+
+  uint64_t* buf = (k_eff <= kSelectSmemCap) ? sbuf : gbuf + row * (uint64_t)gbuf_stride;
+
+  // digit schedule: key32 bits [32+key_bits-1, 32], then id bits [id_bits-1, 0]
+  Digit digits[8];
+  int nd = 0;
+  for (int part = 0; part < 2; part++) {
+    uint32_t bits = part == 0 ? a.key_bits : a.id_bits;
+    uint32_t top = (part == 0 ? 32u : 0u) + bits;
+    while (bits > 0) {
+      uint32_t w = bits < 11 ? bits : 11;
+      top -= w;
+      digits[nd++] = Digit{top, w};
+      bits -= w;
+    }
+  }
+
+  uint64_t prefix = 0, fixed = 0;
+  uint32_t need = k_eff;
+  bool take_all = (k_eff == n);
+  for (int d = 0; d < nd && !take_all; d++) {
+    const uint32_t shift = digits[d].shift, width = digits[d].width;
+    const uint32_t nbins = 1u << width;
+    for (uint32_t b = threadIdx.x; b < kHistBins; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
+    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
+      uint64_t key = load_key(keys, ids, i);
+      if ((key & fixed) == prefix) atomicAdd(&hist[(uint32_t)(key >> shift) & (nbins - 1)], 1u);
+    }
+    __syncthreads();
+    // block scan over bins (2 per thread) to find the bin holding the need-th key
+    const uint32_t t = threadIdx.x;
+    uint32_t h0 = hist[2 * t], h1 = hist[2 * t + 1];
+    uint32_t s = h0 + h1, incl = s;
+    const int lane = t & 31, w = t >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      uint32_t v = warp_tot[lane], x = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+      }
+      warp_tot[lane] = x - v;  // exclusive warp offsets
+    }
+    __syncthreads();
+    uint32_t excl = warp_tot[w] + incl - s;
+    if (excl < need && need <= excl + s) {
+      if (need <= excl + h0) {
+        s_bin = 2 * t;
+        s_before = excl;
+        s_in_bin = h0;
+      } else {
+        s_bin = 2 * t + 1;
+        s_before = excl + h0;
+        s_in_bin = h1;
+      }
+    }
+    __syncthreads();
+    need -= s_before;
+    prefix |= (uint64_t)s_bin << shift;
+    fixed |= (uint64_t)(nbins - 1) << shift;
+    if (s_in_bin == need) take_all = true;  // the whole bin is taken
+    __syncthreads();
+  }
+
+  // collect: keys strictly below the prefix, then `need` keys inside it
+  if (threadIdx.x == 0) {
+    s_cnt_below = 0;
+    s_cnt_tie = 0;
+  }
+  __syncthreads();
+  const uint32_t below_total = k_eff - need;
+  for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    uint64_t key = load_key(keys, ids, i);
+    uint64_t m = key & fixed;
+    if (m < prefix) {
+      uint32_t slot = atomicAdd(&s_cnt_below, 1u);
+      if (slot < below_total) buf[slot] = key;
+    } else if (m == prefix) {
+      uint32_t tk = atomicAdd(&s_cnt_tie, 1u);
+      if (tk < need) buf[below_total + tk] = key;
+    }
+  }
+  __syncthreads();
+  uint32_t len = 1;
+  while (len < k_eff) len <<= 1;
+  for (uint32_t j = k_eff + threadIdx.x; j < len; j += blockDim.x) buf[j] = ~0ull;
+  __syncthreads();
+  bitonic_sort(buf, len);
+  for (uint32_t j = threadIdx.x; j < k_eff; j += blockDim.x) {
+    uint64_t key = buf[j];
+    out_k[j] = (uint32_t)(key >> 32);
+    out_i[j] = (uint32_t)key;
+  }
+}
+
+}  // namespace
+
+size_t select_rows_scratch_elems(uint64_t rows, uint32_t k) {
+  if (k <= kSelectSmemCap) return 0;
+  uint64_t len = 1;
+  while (len < k) len <<= 1;
+  return rows * len;
+}
+
+void launch_select_rows(const SelectArgs& a, uint64_t rows, uint64_t* scratch,
+                        cudaStream_t stream) {
+  if (rows == 0) return;
+  uint32_t stride = 0;
+  if (a.k > kSelectSmemCap) {
+    uint64_t len = 1;
+    while (len < a.k) len <<= 1;
+    stride = (uint32_t)len;
+  }
+  select_rows_kernel<<<(unsigned)rows, kSelThreads, 0, stream>>>(a, scratch, stride);
+  launched();
+}
+
+}  // namespace ovb
