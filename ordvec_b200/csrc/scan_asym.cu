@@ -22,13 +22,20 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Dot product of one u32 word of codes with its query slice.  Each of the CPB
+// code positions of a byte keeps its own FP32 chain of 4 products (short
+// chains keep the rounding error per chain tiny); the chains are combined in
+// FP64 so the cross-word sum meets the 1e-5-relative-of-FP64 contract even for
+// scores near zero, where FP32 cancellation would not.
 template <int BITS>
-__device__ __forceinline__ float word_dot(uint32_t x, const float* q) {
+__device__ __forceinline__ double word_dot(uint32_t x, const float* q) {
   constexpr int CPB = 8 / BITS;
   constexpr uint32_t MASK = (1u << BITS) - 1;
   constexpr float SCALE = (float)(1u << BITS);
   constexpr float OFF = -((float)(1u << BITS) + ((float)(1u << BITS) - 1.0f) * 0.5f);
-  float a0 = 0.0f, a1 = 0.0f;
+  float a[CPB];
+#pragma unroll
+  for (int i = 0; i < CPB; i++) a[i] = 0.0f;
 #pragma unroll
   for (int b = 0; b < 4; b++) {
 #pragma unroll
@@ -37,13 +44,17 @@ __device__ __forceinline__ float word_dot(uint32_t x, const float* q) {
       const uint32_t code = (x >> s) & MASK;
       const float f = __uint_as_float(0x3F800000u | (code << (23 - BITS)));
       const float c = fmaf(f, SCALE, OFF);
-      if (i & 1)
-        a1 = fmaf(q[b * CPB + i], c, a1);
-      else
-        a0 = fmaf(q[b * CPB + i], c, a0);
+      a[i] = fmaf(q[b * CPB + i], c, a[i]);
     }
   }
-  return a0 + a1;
+  double t = 0.0;
+#pragma unroll
+  for (int i = 0; i < CPB; i++) t += (double)a[i];
+  return t;
+}
+
+__device__ __forceinline__ uint32_t score_key(double dot, float inv_norm) {
+  return desc_key((float)(dot * (double)inv_norm));
 }
 
 // G lanes per row, W words per lane (compile time), q in registers.
@@ -59,9 +70,9 @@ __device__ __forceinline__ void load_q(const float* qu, uint32_t words, int g, f
 }
 
 template <int BITS, int G, int W>
-__device__ __forceinline__ float row_dot(const uint32_t* row, uint32_t words, int g,
-                                         const float (&qr)[W][32 / BITS]) {
-  float acc = 0.0f;
+__device__ __forceinline__ double row_dot(const uint32_t* row, uint32_t words, int g,
+                                          const float (&qr)[W][32 / BITS]) {
+  double acc = 0.0;
 #pragma unroll
   for (int i = 0; i < W; i++) {
     const uint32_t w = g + i * G;
@@ -89,8 +100,8 @@ __global__ void __launch_bounds__(kThreads)
   for (uint64_t base = gw * RPW; base < n; base += nw * RPW) {
     const uint64_t doc = base + lane / G;
     const uint64_t rd = doc < n ? doc : n - 1;
-    const float dot = row_dot<BITS, G, W>((const uint32_t*)codes + rd * words, words, g, qr);
-    if (g == 0 && doc < n) out[doc] = desc_key(dot * inv_norm);
+    const double dot = row_dot<BITS, G, W>((const uint32_t*)codes + rd * words, words, g, qr);
+    if (g == 0 && doc < n) out[doc] = score_key(dot, inv_norm);
   }
 }
 
@@ -112,22 +123,22 @@ __global__ void __launch_bounds__(kThreads)
   for (uint64_t base = s + gw * RPW; base < e; base += nw * RPW) {
     const uint64_t i = base + lane / G;
     const uint64_t ri = i < e ? i : e - 1;
-    const float dot = row_dot<BITS, G, W>((const uint32_t*)codes + (uint64_t)cands[ri] * words, words, g, qr);
-    if (g == 0 && i < e) keys[i] = desc_key(dot * inv_norm);
+    const double dot = row_dot<BITS, G, W>((const uint32_t*)codes + (uint64_t)cands[ri] * words, words, g, qr);
+    if (g == 0 && i < e) keys[i] = score_key(dot, inv_norm);
   }
 }
 
 // Generic byte-wise path for rows that are not a whole number of u32 words or
 // too wide for the register path: one warp per row, q read from global.
-__device__ __forceinline__ float generic_row_dot(const uint8_t* row, uint32_t dim, uint32_t bits,
-                                                 const float* qu) {
+__device__ __forceinline__ double generic_row_dot(const uint8_t* row, uint32_t dim, uint32_t bits,
+                                                  const float* qu) {
   const int lane = threadIdx.x & 31;
   const uint32_t cpb = 8 / bits, mask = (1u << bits) - 1;
-  const float centre = ((float)(1u << bits) - 1.0f) * 0.5f;
-  float acc = 0.0f;
+  const double centre = ((double)(1u << bits) - 1.0) * 0.5;
+  double acc = 0.0;
   for (uint32_t j = lane; j < dim; j += 32) {
     const uint32_t code = (row[j / cpb] >> ((cpb - 1 - j % cpb) * bits)) & mask;
-    acc = fmaf(qu[j], (float)code - centre, acc);
+    acc = fma((double)qu[j], (double)code - centre, acc);
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
   return acc;
@@ -142,8 +153,8 @@ __global__ void __launch_bounds__(kThreads)
   const uint64_t gw = ((uint64_t)blockIdx.x * kThreads + threadIdx.x) / 32;
   const uint64_t nw = (uint64_t)gridDim.x * kThreads / 32;
   for (uint64_t doc = gw; doc < n; doc += nw) {
-    const float dot = generic_row_dot(codes + doc * bpv, dim, bits, q_unit + qi * dim);
-    if ((threadIdx.x & 31) == 0) keys[qi * ld + doc] = desc_key(dot * inv_norm);
+    const double dot = generic_row_dot(codes + doc * bpv, dim, bits, q_unit + qi * dim);
+    if ((threadIdx.x & 31) == 0) keys[qi * ld + doc] = score_key(dot, inv_norm);
   }
 }
 
@@ -157,8 +168,8 @@ __global__ void __launch_bounds__(kThreads)
   const uint64_t gw = ((uint64_t)blockIdx.x * kThreads + threadIdx.x) / 32;
   const uint64_t nw = (uint64_t)gridDim.x * kThreads / 32;
   for (uint64_t i = off[qi] + gw; i < off[qi + 1]; i += nw) {
-    const float dot = generic_row_dot(codes + (uint64_t)cands[i] * bpv, dim, bits, q_unit + qi * dim);
-    if ((threadIdx.x & 31) == 0) keys[i] = desc_key(dot * inv_norm);
+    const double dot = generic_row_dot(codes + (uint64_t)cands[i] * bpv, dim, bits, q_unit + qi * dim);
+    if ((threadIdx.x & 31) == 0) keys[i] = score_key(dot, inv_norm);
   }
 }
 
