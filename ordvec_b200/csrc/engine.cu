@@ -115,7 +115,7 @@ uint32_t engine_rankquant_subset(const Index& rq, const float* d_q, uint64_t nq,
 
 // Stage-1 candidates into w.sel_keys / w.sel_ids, rows of m_eff ids.
 uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint64_t m,
-                           const float* d_weights, Workspace& w, cudaStream_t st) {
+                           const float* d_weights, Workspace& w, cudaStream_t st, const float* q_unit) {
   const uint32_t me = (uint32_t)(m < s1.n ? m : s1.n);
   if (!me || !nq) return me;
   uint32_t* sk = (uint32_t*)w.sel_keys.ensure(nq * me * 4);
@@ -139,7 +139,7 @@ uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint6
       break;
     }
     case OVB_INDEX_KIND_FASTSCAN: {
-      const float* qu = normalised(w, d_q, nq, s1.dim, st);
+      const float* qu = q_unit ? q_unit : normalised(w, d_q, nq, s1.dim, st);
       uint8_t* lut = (uint8_t*)w.lut.ensure(nq * s1.pairs_pad * 16);
       float* bias = (float*)w.bias.ensure(nq * 4);
       float* invq = (float*)w.invq.ensure(nq * 4);
@@ -210,12 +210,13 @@ uint32_t engine_two_stage(const Index& rq, const Index& s1, const float* d_q, ui
   if (s1.n != rq.n) fail(ORDVEC_STATUS_BAD_ARGUMENT, "stage-1 index len must match RankQuant len");
   const uint64_t m_req = m ? m : default_candidate_count(k, rq.n);
   w.mark(st, 0);
-  const uint32_t me = engine_candidates(s1, d_q, nq, m_req, nullptr, w, st);
+  if (!nq) return 0;
+  const float* qu = normalised(w, d_q, nq, rq.dim, st);  // shared by both stages
+  const uint32_t me = engine_candidates(s1, d_q, nq, m_req, nullptr, w, st, qu);
   const uint32_t ke = (uint32_t)(k < me ? k : me);
-  if (!ke || !nq) return ke;
+  if (!ke) return ke;
   uint64_t* off = (uint64_t*)w.off.ensure((nq + 1) * 8);
   launch_uniform_offsets(off, nq, me, st);
-  const float* qu = normalised(w, d_q, nq, rq.dim, st);
   const float inv_norm = inv_rankquant_norm(rq.dim, rq.bits);
   uint32_t* keys = (uint32_t*)w.keys2.ensure(nq * me * 4);
   launch_asym_subset(rq.codes.as<uint8_t>(), rq.dim, rq.bits, qu, nq, off, w.sel_ids.as<uint32_t>(), me,

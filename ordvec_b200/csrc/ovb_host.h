@@ -119,7 +119,8 @@ uint32_t engine_rankquant_subset(const Index& rq, const float* d_q, uint64_t nq,
                                  const uint64_t* d_off, const uint32_t* d_cands, uint64_t max_row,
                                  uint64_t k, Workspace& w, cudaStream_t st);
 uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint64_t m,
-                           const float* d_weights, Workspace& w, cudaStream_t st);
+                           const float* d_weights, Workspace& w, cudaStream_t st,
+                           const float* q_unit = nullptr);
 uint32_t engine_bitmap_full(const Index& bm, const float* d_q, uint64_t nq, uint64_t k,
                             Workspace& w, cudaStream_t st);
 uint32_t engine_fastscan_full(const Index& fs, const float* d_q, uint64_t nq, uint64_t k,

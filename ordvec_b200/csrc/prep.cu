@@ -19,16 +19,36 @@ namespace ovb {
 
 namespace {
 
+// One warp per query.  The warp squares the query into shared memory in
+// 1024-element chunks; lane 0 then adds the squares in index order (the
+// reference's sequential f32 sum) with loads four at a time, so the chain is
+// bound by the add latency, not by memory latency.
 __global__ void l2_normalise_kernel(const float* __restrict__ q, uint64_t nq, uint32_t dim,
                                     float* __restrict__ out) {
-  const uint64_t qi = (uint64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  __shared__ __align__(16) float sq[8][1024];
+  const int wid = threadIdx.x / 32;
+  const uint64_t qi = (uint64_t)blockIdx.x * (blockDim.x / 32) + wid;
   const int lane = threadIdx.x & 31;
   if (qi >= nq) return;
   const float* x = q + qi * dim;
   float* y = out + qi * dim;
   float s = -0.0f;
-  if (lane == 0) {
-    for (uint32_t j = 0; j < dim; j++) s = __fadd_rn(s, __fmul_rn(x[j], x[j]));
+  for (uint32_t c0 = 0; c0 < dim; c0 += 1024) {
+    const uint32_t cn = dim - c0 < 1024 ? dim - c0 : 1024;
+    for (uint32_t j = lane; j < cn; j += 32) sq[wid][j] = __fmul_rn(x[c0 + j], x[c0 + j]);
+    __syncwarp();
+    if (lane == 0) {
+      uint32_t j = 0;
+      for (; j + 4 <= cn; j += 4) {
+        const float4 v = *reinterpret_cast<const float4*>(&sq[wid][j]);
+        s = __fadd_rn(s, v.x);
+        s = __fadd_rn(s, v.y);
+        s = __fadd_rn(s, v.z);
+        s = __fadd_rn(s, v.w);
+      }
+      for (; j < cn; j++) s = __fadd_rn(s, sq[wid][j]);
+    }
+    __syncwarp();
   }
   s = __shfl_sync(0xFFFFFFFFu, s, 0);
   const float norm = __fsqrt_rn(s);

@@ -13,6 +13,8 @@
 // still match the fixed prefix, finds the bin holding the k-th key, and stops
 // as soon as that bin holds exactly the keys still needed.  A collect pass
 // then gathers the k winners and a bitonic sort orders them.
+#include <cooperative_groups.h>
+
 #include "ovb_common.cuh"
 #include "ovb_kernels.h"
 
@@ -181,6 +183,158 @@ __global__ void __launch_bounds__(kSelThreads)
   }
 }
 
+// Cluster form for few long rows (the one-query-per-launch path): a cluster of
+// kClusterCtas CTAs shares one row.  Each CTA histograms its contiguous slice;
+// the per-CTA histograms are summed through distributed shared memory, every
+// CTA derives the same bin, and the winners are gathered into CTA 0's shared
+// memory, which sorts and writes them.  All waits are hardware cluster
+// barriers.
+constexpr int kClusterCtas = 8;
+constexpr uint32_t kClusterCap = 2048;
+
+__global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kSelThreads)
+    select_rows_cluster_kernel(SelectArgs a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  __shared__ uint32_t hist[kHistBins];
+  __shared__ uint32_t tot[kHistBins];
+  __shared__ uint32_t warp_tot[kSelThreads / 32];
+  __shared__ uint64_t sbuf[kClusterCap];
+  __shared__ uint32_t s_bin, s_before, s_in_bin, s_cnt_below, s_cnt_tie;
+
+  const uint32_t crank = cluster.block_rank();
+  const uint64_t row = blockIdx.x / kClusterCtas;
+  uint64_t start, n;
+  if (a.row_off) {
+    start = a.row_off[row];
+    n = a.row_off[row + 1] - start;
+  } else {
+    start = row * a.ld;
+    n = a.n;
+  }
+  const uint32_t* keys = a.keys + start;
+  const uint32_t* ids = a.ids ? a.ids + start : nullptr;
+  const uint32_t k_eff = (uint32_t)(n < a.k ? n : a.k);
+  const uint64_t per = (n + kClusterCtas - 1) / kClusterCtas;
+  const uint64_t lo = crank * per < n ? crank * per : n;
+  const uint64_t hi = lo + per < n ? lo + per : n;
+
+  Digit digits[8];
+  int nd = 0;
+  for (int part = 0; part < 2; part++) {
+    uint32_t bits = part == 0 ? a.key_bits : a.id_bits;
+    uint32_t top = (part == 0 ? 32u : 0u) + bits;
+    while (bits > 0) {
+      uint32_t w = bits < 11 ? bits : 11;
+      top -= w;
+      digits[nd++] = Digit{top, w};
+      bits -= w;
+    }
+  }
+
+  uint64_t prefix = 0, fixed = 0;
+  uint32_t need = k_eff;
+  bool take_all = (k_eff == n);
+  for (int d = 0; d < nd && !take_all && k_eff > 0; d++) {
+    const uint32_t shift = digits[d].shift, width = digits[d].width;
+    const uint32_t nbins = 1u << width;
+    for (uint32_t b = threadIdx.x; b < kHistBins; b += blockDim.x) hist[b] = 0;
+    cluster.sync();
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      uint64_t key = load_key(keys, ids, i);
+      if ((key & fixed) == prefix) atomicAdd(&hist[(uint32_t)(key >> shift) & (nbins - 1)], 1u);
+    }
+    cluster.sync();
+    for (uint32_t b = threadIdx.x; b < kHistBins; b += blockDim.x) {
+      uint32_t s = 0;
+      for (int r = 0; r < kClusterCtas; r++) s += cluster.map_shared_rank(hist, r)[b];
+      tot[b] = s;
+    }
+    __syncthreads();
+    const uint32_t t = threadIdx.x;
+    uint32_t h0 = tot[2 * t], h1 = tot[2 * t + 1];
+    uint32_t s = h0 + h1, incl = s;
+    const int lane = t & 31, w = t >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      uint32_t v = warp_tot[lane], x = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+      }
+      warp_tot[lane] = x - v;
+    }
+    __syncthreads();
+    uint32_t excl = warp_tot[w] + incl - s;
+    if (excl < need && need <= excl + s) {
+      if (need <= excl + h0) {
+        s_bin = 2 * t;
+        s_before = excl;
+        s_in_bin = h0;
+      } else {
+        s_bin = 2 * t + 1;
+        s_before = excl + h0;
+        s_in_bin = h1;
+      }
+    }
+    __syncthreads();
+    need -= s_before;
+    prefix |= (uint64_t)s_bin << shift;
+    fixed |= (uint64_t)(nbins - 1) << shift;
+    if (s_in_bin == need) take_all = true;
+    // no CTA may reset its histogram while another still reads it
+    cluster.sync();
+  }
+
+  uint32_t* out_k = a.out_keys + row * (uint64_t)a.k;
+  uint32_t* out_i = a.out_ids + row * (uint64_t)a.k;
+  if (crank == 0) {
+    for (uint32_t j = k_eff + threadIdx.x; j < a.k; j += blockDim.x) {
+      out_k[j] = kSentinelKey;
+      out_i[j] = kSentinelId;
+    }
+    if (threadIdx.x == 0) {
+      s_cnt_below = 0;
+      s_cnt_tie = 0;
+    }
+  }
+  cluster.sync();
+  const uint32_t below_total = k_eff - need;
+  uint64_t* buf0 = cluster.map_shared_rank(sbuf, 0);
+  uint32_t* below0 = cluster.map_shared_rank(&s_cnt_below, 0);
+  uint32_t* tie0 = cluster.map_shared_rank(&s_cnt_tie, 0);
+  if (k_eff > 0) {
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      uint64_t key = load_key(keys, ids, i);
+      uint64_t m = key & fixed;
+      if (m < prefix) {
+        uint32_t slot = atomicAdd(below0, 1u);
+        if (slot < below_total) buf0[slot] = key;
+      } else if (m == prefix) {
+        uint32_t tk = atomicAdd(tie0, 1u);
+        if (tk < need) buf0[below_total + tk] = key;
+      }
+    }
+  }
+  cluster.sync();
+  if (crank == 0 && k_eff > 0) {
+    uint32_t len = 1;
+    while (len < k_eff) len <<= 1;
+    for (uint32_t j = k_eff + threadIdx.x; j < len; j += blockDim.x) sbuf[j] = ~0ull;
+    __syncthreads();
+    bitonic_sort(sbuf, len);
+    for (uint32_t j = threadIdx.x; j < k_eff; j += blockDim.x) {
+      out_k[j] = (uint32_t)(sbuf[j] >> 32);
+      out_i[j] = (uint32_t)sbuf[j];
+    }
+  }
+}
+
 }  // namespace
 
 size_t select_rows_scratch_elems(uint64_t rows, uint32_t k) {
@@ -193,6 +347,12 @@ size_t select_rows_scratch_elems(uint64_t rows, uint32_t k) {
 void launch_select_rows(const SelectArgs& a, uint64_t rows, uint64_t* scratch,
                         cudaStream_t stream) {
   if (rows == 0) return;
+  // few long rows: one 8-CTA cluster per row
+  if (!a.row_off && a.k <= kClusterCap && a.n >= 32768 && rows * kClusterCtas <= 2 * 148) {
+    select_rows_cluster_kernel<<<(unsigned)(rows * kClusterCtas), kSelThreads, 0, stream>>>(a);
+    launched();
+    return;
+  }
   uint32_t stride = 0;
   if (a.k > kSelectSmemCap) {
     uint64_t len = 1;
