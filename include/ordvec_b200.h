@@ -227,6 +227,19 @@ ordvec_status_t ovb_two_stage_profile(const ordvec_index_t *rq, const ordvec_ind
                                       const float *d_queries, uint64_t nq, uint64_t m,
                                       uint64_t k, float *d_scores, int64_t *d_ids, void *stream,
                                       float *stage_ms);
+/* Allocation-free RankQuant full search (no counterpart in the reference):
+ * same results as ovb_rankquant_search, but device pointers in and out,
+ * asynchronous on `stream`, and no device allocation at all -- for callers
+ * that may not call cudaMalloc (latency-bound serving threads, processes whose
+ * device memory belongs to one budgeted allocator).  Intermediates live in a
+ * fixed 32 MiB device array inside this library (held by every GPU that loads
+ * it): requests needing more (nq*dim*4 + nq*n*4 + 2*nq*k*4 bytes, each part
+ * rounded up to 256) or k > 4096 are rejected with BAD_ARGUMENT.  The first
+ * call on a device looks up the array's device address; make it before any
+ * stream capture.  Calls that overlap on the GPU share the array and race. */
+ordvec_status_t ovb_rankquant_search_noalloc(const ordvec_index_t *rq, const float *d_queries,
+                                             uint64_t nq, uint64_t k, float *d_scores,
+                                             int64_t *d_ids, void *stream);
 /* Number of kernel launches the last device/host search on this thread
  * issued (instrumentation for benchmarks). */
 uint64_t ovb_last_launch_count(void);

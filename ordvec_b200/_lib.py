@@ -99,6 +99,7 @@ SIGNATURES = {
     "ovb_two_stage_search": (S, [P, P, P, U64, U64, U64, P, P]),
     "ovb_two_stage_search_device": (S, [P, P, P, U64, U64, U64, P, P, P]),
     "ovb_two_stage_profile": (S, [P, P, P, U64, U64, U64, P, P, P, P]),
+    "ovb_rankquant_search_noalloc": (S, [P, P, U64, U64, P, P, P]),
     "ovb_last_launch_count": (U64, []),
     "ovb_set_device": (S, [C.c_int]),
     "ovb_synth_docs": (S, [U64, U64, U64, U32, F, P]),

@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
 
 #include "ovb_host.h"
 
@@ -179,6 +180,8 @@ uint32_t bitmap_subset(const Index& bm, const float* d_q, uint64_t nq, const uin
 }
 
 }  // namespace
+
+ordvec_status_t api_boundary(const std::function<void()>& f) { return boundary(f); }
 
 Workspace::Workspace() {
   OVB_CUDA(cudaGetDevice(&device));
