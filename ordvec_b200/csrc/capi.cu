@@ -147,6 +147,21 @@ const float* upload_queries(Workspace& w, const float* q, uint64_t nq, uint32_t 
   return d;
 }
 
+// After a synchronised pipeline: surface a timed-out wait of a tensor-core
+// kernel (its results are then incomplete) as INTERNAL, and re-arm the word.
+void check_tc(Workspace& w) {
+  if (!w.tc_used) return;
+  w.tc_used = false;
+  uint32_t* h = (uint32_t*)w.pinned.ensure(4);
+  OVB_CUDA(cudaMemcpyAsync(h, w.tc_err.p, 4, cudaMemcpyDeviceToHost, w.stream));
+  OVB_CUDA(cudaStreamSynchronize(w.stream));
+  if (*h) {
+    OVB_CUDA(cudaMemsetAsync(w.tc_err.p, 0, 4, w.stream));
+    OVB_CUDA(cudaStreamSynchronize(w.stream));
+    fail(ORDVEC_STATUS_INTERNAL, "tensor-core FastScan scan: a bounded wait timed out; results discarded");
+  }
+}
+
 // results of the last pipeline (w.out_keys / w.out_ids, count entries) -> host
 void download_results(Workspace& w, uint64_t count, int mode, uint32_t n_top, float* scores, int64_t* ids) {
   if (!count) return;
@@ -156,6 +171,7 @@ void download_results(Workspace& w, uint64_t count, int mode, uint32_t n_top, fl
   OVB_CUDA(cudaMemcpyAsync(scores, ds, count * 4, cudaMemcpyDeviceToHost, w.stream));
   OVB_CUDA(cudaMemcpyAsync(ids, di, count * 8, cudaMemcpyDeviceToHost, w.stream));
   OVB_CUDA(cudaStreamSynchronize(w.stream));
+  check_tc(w);
 }
 
 void need_queries(const float* q, uint64_t nq) {
@@ -643,6 +659,7 @@ static void top_m_host(const Index& ix, const float* queries, uint64_t nq, uint6
   uint32_t got = engine_candidates(ix, d_q, nq, me, d_w, w, w.stream);
   OVB_CUDA(cudaMemcpyAsync(out, w.sel_ids.p, nq * got * 4, cudaMemcpyDeviceToHost, w.stream));
   OVB_CUDA(cudaStreamSynchronize(w.stream));
+  check_tc(w);
 }
 
 ordvec_status_t ovb_sign_bitmap_top_m(const ordvec_index_t* sign, const float* queries, uint64_t nq, uint64_t m,
@@ -782,6 +799,8 @@ ordvec_status_t ovb_two_stage_profile(const ordvec_index_t* rq, const ordvec_ind
     w.prof = false;
     OVB_CUDA(cudaStreamSynchronize(st));
     for (int i = 0; i < 5; i++) OVB_CUDA(cudaEventElapsedTime(&stage_ms[i], w.prof_ev[i], w.prof_ev[i + 1]));
+    OVB_CUDA(cudaStreamSynchronize(w.stream));
+    check_tc(w);
   });
 }
 

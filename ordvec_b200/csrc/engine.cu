@@ -65,6 +65,15 @@ float* normalised(Workspace& w, const float* d_q, uint64_t nq, uint32_t dim, cud
   return qu;
 }
 
+// Tensor-core FastScan for batches of at least 32 queries (one tile of the
+// one-hot GEMM needs N >= 16 and pays off from ~32); OVB_FASTSCAN_TC=0/1 forces.
+bool use_fastscan_tc(uint64_t nq) {
+  const char* e = getenv("OVB_FASTSCAN_TC");
+  if (e && e[0] == '0') return false;
+  if (e && e[0] == '1') return true;
+  return nq >= 32;
+}
+
 void require_kind(const Index& ix, uint32_t kind, const char* what) {
   if (ix.kind != kind) fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, std::string(what) + ": wrong index kind");
 }
@@ -147,8 +156,12 @@ uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint6
       w.mark(st, 1);
       const float inv_norm = inv_rankquant_norm(s1.dim, 2);
       full_scan_select(w, nq, n, me, 32, sk, si, st, [&](uint64_t q0, uint64_t qn, uint32_t* keys) {
-        launch_fastscan_scan(s1.codes.as<uint8_t>(), n, s1.pairs_pad, lut + q0 * s1.pairs_pad * 16, bias + q0,
-                             invq + q0, inv_norm, qn, keys, n, st);
+        if (use_fastscan_tc(qn))
+          launch_fastscan_scan_tc(s1.codes.as<uint8_t>(), n, s1.pairs_pad, lut + q0 * s1.pairs_pad * 16,
+                                  bias + q0, invq + q0, inv_norm, qn, keys, n, w.tc_err_word(st), st);
+        else
+          launch_fastscan_scan(s1.codes.as<uint8_t>(), n, s1.pairs_pad, lut + q0 * s1.pairs_pad * 16, bias + q0,
+                               invq + q0, inv_norm, qn, keys, n, st);
       });
       break;
     }

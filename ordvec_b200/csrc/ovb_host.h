@@ -97,6 +97,17 @@ struct Workspace {
   DevBuf q_raw, q_unit, qbits, lut, bias, invq, keys, sel_keys, sel_ids, off, keys2, out_keys,
       out_ids, scores, ids, scratch, stage, weights, flag;
   HostBuf pinned;
+  // error word of the tensor-core kernels (zeroed once; checked by host APIs)
+  DevBuf tc_err;
+  bool tc_used = false;
+  uint32_t* tc_err_word(cudaStream_t st) {
+    if (!tc_err.p) {
+      tc_err.ensure(4);
+      OVB_CUDA(cudaMemsetAsync(tc_err.p, 0, 4, st));
+    }
+    tc_used = true;
+    return tc_err.as<uint32_t>();
+  }
   // stage markers for ovb_two_stage_profile (recorded only while prof is set)
   cudaEvent_t prof_ev[6] = {};
   bool prof = false;

@@ -59,6 +59,11 @@ void launch_fastscan_scan(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad,
                           const uint8_t* lut, const float* bias_sum, const float* inv_q,
                           float inv_norm, uint64_t nq, uint32_t* keys, uint64_t ld,
                           cudaStream_t stream);
+// Tensor-core form (scan_fastscan_tc.cu): same keys, bit for bit; *err (device
+// u32) gets bit 0 set if a bounded wait timed out.
+void launch_fastscan_scan_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad, const uint8_t* lut,
+                             const float* bias_sum, const float* inv_q, float inv_norm, uint64_t nq,
+                             uint32_t* keys, uint64_t ld, uint32_t* err, cudaStream_t stream);
 void launch_fastscan_relayout(const uint8_t* ref_blocks, uint64_t n, uint32_t pairs,
                               uint32_t pairs_pad, uint8_t* dev_blocks, cudaStream_t stream);
 

@@ -248,9 +248,12 @@ void launch_asym_subset(const uint8_t* codes, uint32_t dim, uint32_t bits, const
                         uint64_t max_row, float inv_norm, uint32_t* keys, cudaStream_t stream) {
   if (!nq || !max_row) return;
   const int W = plan_w(dim, bits);
+  // each warp loads its query slice once, so give it ~32 rows when there are
+  // many queries; a single query spreads its rows over more CTAs
+  const uint64_t rows_per_warp = nq >= 64 ? 32 : 4;
   for (uint64_t q0 = 0; q0 < nq; q0 += 65535) {
     unsigned gy = (unsigned)((nq - q0) < 65535 ? (nq - q0) : 65535);
-    dim3 grid(grid_x(kThreads / 32, max_row), gy);
+    dim3 grid(grid_x((kThreads / 32) * rows_per_warp, max_row), gy);
     if (W)
       dispatch(bits, W, true, grid, stream, codes, 0, dim, q_unit + q0 * dim, inv_norm, keys, 0, offsets + q0,
                cands);

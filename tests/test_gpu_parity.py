@@ -353,6 +353,26 @@ def test_fastscan_search_is_bit_exact(orc, dim, n):
     assert np.array_equal(res.scores.reshape(5, k).view(np.uint32), s_ref.view(np.uint32))
 
 
+@pytest.mark.parametrize("dim,n,nq", [(100, 777, 40), (1024, 5000, 300), (64, 65, 33)])
+def test_fastscan_tensor_core_path_is_bit_exact(orc, monkeypatch, dim, n, nq):
+    """The tcgen05 one-hot GEMM form (>= 32 queries) against the oracle and the
+    CUDA-core form: identical ids and score bits, partial query tiles included."""
+    docs = ob.synth_docs(23, n, dim)
+    queries, _ = ob.synth_queries(23, n, nq, dim)
+    fs = ob.RankQuantFastscan(dim)
+    fs.add(docs)
+    k = min(100, n)
+    monkeypatch.setenv("OVB_FASTSCAN_TC", "1")
+    tc = fs.search(queries, k)
+    monkeypatch.setenv("OVB_FASTSCAN_TC", "0")
+    cc = fs.search(queries, k)
+    assert np.array_equal(tc.indices, cc.indices)
+    assert np.array_equal(tc.scores.view(np.uint32), cc.scores.view(np.uint32))
+    s_ref, i_ref = orc.fastscan_search(orc.fastscan_pack(docs, dim), n, dim, queries[:4], k)
+    assert np.array_equal(tc.indices.reshape(nq, k)[:4], i_ref)
+    assert np.array_equal(tc.scores.reshape(nq, k)[:4].view(np.uint32), s_ref.view(np.uint32))
+
+
 def test_fastscan_reference_formula_corpus(orc):
     """src/fastscan.rs:755-777 corpus (dim 64, n 65, k 9) including a zero query."""
     dim, n, k = 64, 65, 9
