@@ -220,9 +220,10 @@ ordvec_status_t ovb_two_stage_search_device(const ordvec_index_t *rq,
                                             uint64_t k, float *d_scores, int64_t *d_ids,
                                             void *stream);
 /* Same as ovb_two_stage_search_device, synchronous, with CUDA events recorded
- * on `stream` between the pipeline stages; stage_ms[0..4] receives the device
- * time of: query prep, stage-1 scan, stage-1 select, rerank scoring, final
- * select (benchmark instrumentation). */
+ * on `stream` between the pipeline stages; stage_ms[0..5] receives the device
+ * time of: query prep, stage-1 candidate threshold (sample scan + select; 0
+ * when the stage-1 scan keeps its full key matrix), stage-1 scan, stage-1
+ * select, rerank scoring, final select (benchmark instrumentation). */
 ordvec_status_t ovb_two_stage_profile(const ordvec_index_t *rq, const ordvec_index_t *stage1,
                                       const float *d_queries, uint64_t nq, uint64_t m,
                                       uint64_t k, float *d_scores, int64_t *d_ids, void *stream,

@@ -432,8 +432,9 @@ def two_stage_search_device(rq: RankQuant, stage1: _Index, d_queries: int, nq: i
 def two_stage_profile(rq: RankQuant, stage1: _Index, d_queries: int, nq: int, m: int, k: int,
                       d_scores: int, d_ids: int, stream: int) -> List[float]:
     """Synchronous device-pointer two-stage search returning per-stage device ms:
-    [prep, stage-1 scan, stage-1 select, rerank scoring, final select]."""
-    ms = (C.c_float * 5)()
+    [prep, stage-1 threshold, stage-1 scan, stage-1 select, rerank scoring,
+    final select]."""
+    ms = (C.c_float * 6)()
     check(lib().ovb_two_stage_profile(rq.handle, stage1.handle, C.c_void_p(d_queries), nq, m, k,
                                       C.c_void_p(d_scores), C.c_void_p(d_ids), C.c_void_p(stream), ms))
     return list(ms)

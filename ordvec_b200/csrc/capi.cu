@@ -780,7 +780,7 @@ ordvec_status_t ovb_two_stage_profile(const ordvec_index_t* rq, const ordvec_ind
     const Index& s = as_index(stage1);
     need_queries(d_queries, nq);
     if (!stage_ms) fail(ORDVEC_STATUS_NULL_POINTER, "stage_ms pointer is NULL");
-    for (int i = 0; i < 5; i++) stage_ms[i] = 0.0f;
+    for (int i = 0; i < 6; i++) stage_ms[i] = 0.0f;
     if (!nq || !k || !r.n) return;
     if (!d_scores || !d_ids) fail(ORDVEC_STATUS_NULL_POINTER, "output pointer is NULL");
     Workspace& w = workspace();
@@ -798,7 +798,10 @@ ordvec_status_t ovb_two_stage_profile(const ordvec_index_t* rq, const ordvec_ind
     }
     w.prof = false;
     OVB_CUDA(cudaStreamSynchronize(st));
-    for (int i = 0; i < 5; i++) OVB_CUDA(cudaEventElapsedTime(&stage_ms[i], w.prof_ev[i], w.prof_ev[i + 1]));
+    // event order: 0 start, 1 prep, 6 threshold, 2 scan, 3 select, 4 rerank, 5 final
+    static const int order[7] = {0, 1, 6, 2, 3, 4, 5};
+    for (int i = 0; i < 6; i++)
+      OVB_CUDA(cudaEventElapsedTime(&stage_ms[i], w.prof_ev[order[i]], w.prof_ev[order[i + 1]]));
     OVB_CUDA(cudaStreamSynchronize(w.stream));
     check_tc(w);
   });

@@ -32,8 +32,9 @@ float inv_rankquant_norm(uint32_t dim, uint32_t bits) {
 
 void select_rows(Workspace& w, const uint32_t* keys, const uint32_t* ids, const uint64_t* row_off,
                  uint64_t ld, uint64_t n, uint64_t rows, uint32_t k, uint32_t key_bits,
-                 uint32_t id_bits, uint32_t* out_keys, uint32_t* out_ids, cudaStream_t st) {
-  SelectArgs a{keys, ids, row_off, ld, n, k, key_bits, id_bits, out_keys, out_ids};
+                 uint32_t id_bits, uint32_t* out_keys, uint32_t* out_ids, cudaStream_t st,
+                 const uint32_t* row_len = nullptr) {
+  SelectArgs a{keys, ids, row_off, ld, n, k, key_bits, id_bits, out_keys, out_ids, row_len};
   size_t se = select_rows_scratch_elems(rows, k);
   uint64_t* scratch = se ? (uint64_t*)w.scratch.ensure(se * 8) : nullptr;
   launch_select_rows(a, rows, scratch, st);
@@ -72,6 +73,45 @@ bool use_fastscan_tc(uint64_t nq) {
   if (e && e[0] == '0') return false;
   if (e && e[0] == '1') return true;
   return nq >= 32;
+}
+
+// Exact threshold filter for batched FastScan candidate generation (m << n).
+//  1. score an evenly spread sample (every `stride`-th 32-doc block) and take,
+//     per query, the r-th smallest sample key as the threshold thr;
+//  2. rescore every doc, keeping only (key, doc) with key <= thr;
+//  3. a query that kept c docs with m <= c <= cap kept every key <= its m-th
+//     smallest key (at least m keys are <= thr), so the top-m of the kept set,
+//     ties by doc id included, is the top-m of the whole index.  A chunk where
+//     some query kept fewer than m or more than cap docs is redone through the
+//     full key matrix.
+// r is sized so a query keeps about `mult` * m docs (default 3): fewer than m
+// would need the sample to over-represent the top-m ~3x, which for the default
+// sample (>= 8192 docs) is a many-sigma event; the fallback keeps it exact.
+struct FilterPlan {
+  uint32_t stride;
+  uint64_t n_s;
+  uint32_t r;
+  uint32_t cap;
+};
+
+bool filter_plan(uint64_t n, uint32_t m, FilterPlan& p) {
+  const char* e = getenv("OVB_FASTSCAN_FILTER");
+  if (e && e[0] == '0') return false;
+  const bool force = e && e[0] == '1';
+  if (!m || !n || (!force && (n < 32768 || (uint64_t)m * 32 > n))) return false;
+  uint32_t stride = 1;
+  while (stride < 64 && n / (2ull * stride) >= 8192) stride <<= 1;
+  const uint64_t n_s = fastscan_tc_sample_docs(n, stride);
+  const char* me = getenv("OVB_FASTSCAN_SAMPLE_MULT");
+  const double mult = me ? strtod(me, nullptr) : 3.0;
+  double rr = std::ceil(mult * (double)m * (double)n_s / (double)n) + (me ? 0.0 : 16.0);
+  if (rr < 1.0) rr = 1.0;
+  if (rr > (double)n_s) rr = (double)n_s;
+  p.stride = stride;
+  p.n_s = n_s;
+  p.r = (uint32_t)rr;
+  p.cap = (uint32_t)((8ull * m + 2048 + 31) / 32 * 32);
+  return true;
 }
 
 void require_kind(const Index& ix, uint32_t kind, const char* what) {
@@ -140,6 +180,7 @@ uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint6
       else
         launch_bitmap_query(d_q, nq, s1.dim, s1.n_top, qb, st);
       w.mark(st, 1);
+      w.mark(st, 6);  // no sampling stage
       const uint32_t key_bits = bits_for(mode == 0 ? s1.dim : s1.n_top);
       full_scan_select(w, nq, n, me, key_bits, sk, si, st, [&](uint64_t q0, uint64_t qn, uint32_t* keys) {
         launch_popc_scan(mode, s1.codes.as<uint64_t>(), n, s1.qpv(), qb + q0 * s1.qpv(), qn, s1.n_top, keys,
@@ -155,14 +196,62 @@ uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint6
       launch_fastscan_lut(qu, nq, s1.dim, s1.pairs_pad, lut, bias, invq, st);
       w.mark(st, 1);
       const float inv_norm = inv_rankquant_norm(s1.dim, 2);
-      full_scan_select(w, nq, n, me, 32, sk, si, st, [&](uint64_t q0, uint64_t qn, uint32_t* keys) {
-        if (use_fastscan_tc(qn))
-          launch_fastscan_scan_tc(s1.codes.as<uint8_t>(), n, s1.pairs_pad, lut + q0 * s1.pairs_pad * 16,
-                                  bias + q0, invq + q0, inv_norm, qn, keys, n, w.tc_err_word(st), st);
-        else
-          launch_fastscan_scan(s1.codes.as<uint8_t>(), n, s1.pairs_pad, lut + q0 * s1.pairs_pad * 16, bias + q0,
-                               invq + q0, inv_norm, qn, keys, n, st);
-      });
+      const uint8_t* codes = s1.codes.as<uint8_t>();
+      const uint64_t lut_row = (uint64_t)s1.pairs_pad * 16;
+      // rows [qa, qa + qn) through the full key matrix
+      auto dense_rows = [&](uint64_t qa, uint64_t qn) {
+        full_scan_select(w, qn, n, me, 32, sk + qa * me, si + qa * me, st,
+                         [&](uint64_t q0, uint64_t qm, uint32_t* keys) {
+                           const uint64_t qg = qa + q0;
+                           if (use_fastscan_tc(qm))
+                             launch_fastscan_scan_tc(codes, n, s1.pairs_pad, lut + qg * lut_row, bias + qg,
+                                                     invq + qg, inv_norm, qm, 1, keys, n, w.tc_err_word(st), st);
+                           else
+                             launch_fastscan_scan(codes, n, s1.pairs_pad, lut + qg * lut_row, bias + qg, invq + qg,
+                                                  inv_norm, qm, keys, n, st);
+                         });
+      };
+      FilterPlan fp;
+      if (!use_fastscan_tc(nq) || !filter_plan(n, me, fp)) {
+        w.mark(st, 6);  // no sampling stage
+        dense_rows(0, nq);
+        break;
+      }
+      const uint64_t per_q = fp.n_s * 4 + (uint64_t)fp.r * 8 + (uint64_t)fp.cap * 8 + 4;
+      uint64_t qc = keys_budget() / per_q;
+      if (qc < 1) qc = 1;
+      if (qc > nq) qc = nq;
+      uint32_t* smp = (uint32_t*)w.smp_keys.ensure(qc * fp.n_s * 4);
+      uint32_t* tk = (uint32_t*)w.thr_keys.ensure(qc * fp.r * 4);
+      uint32_t* ti = (uint32_t*)w.thr_ids.ensure(qc * fp.r * 4);
+      uint32_t* fk = (uint32_t*)w.f_keys.ensure(qc * fp.cap * 4);
+      uint32_t* fi = (uint32_t*)w.f_ids.ensure(qc * fp.cap * 4);
+      uint32_t* cnt = (uint32_t*)w.f_cnt.ensure(qc * 4);
+      uint32_t* flag = (uint32_t*)w.f_flag.ensure(4);
+      uint32_t* flag_h = (uint32_t*)w.f_flag_host.ensure(4);
+      uint32_t* err = w.tc_err_word(st);
+      for (uint64_t q0 = 0; q0 < nq; q0 += qc) {
+        const uint64_t qn = nq - q0 < qc ? nq - q0 : qc;
+        launch_fastscan_scan_tc(codes, n, s1.pairs_pad, lut + q0 * lut_row, bias + q0, invq + q0, inv_norm, qn,
+                                fp.stride, smp, fp.n_s, err, st);
+        select_rows(w, smp, nullptr, nullptr, fp.n_s, fp.n_s, qn, fp.r, 32, bits_for(fp.n_s - 1), tk, ti, st);
+        w.mark(st, 6);
+        OVB_CUDA(cudaMemsetAsync(cnt, 0, qn * 4, st));
+        OVB_CUDA(cudaMemsetAsync(flag, 0, 4, st));
+        launch_fastscan_filter_tc(codes, n, s1.pairs_pad, lut + q0 * lut_row, bias + q0, invq + q0, inv_norm, qn,
+                                  tk + (fp.r - 1), fp.r, cnt, fp.cap, fk, fi, err, st);
+        launch_filter_check(cnt, qn, me, fp.cap, flag, st);
+        OVB_CUDA(cudaMemcpyAsync(flag_h, flag, 4, cudaMemcpyDeviceToHost, st));
+        OVB_CUDA(cudaStreamSynchronize(st));
+        if (*flag_h) {
+          dense_rows(q0, qn);
+          continue;
+        }
+        w.mark(st, 2);
+        select_rows(w, fk, fi, nullptr, fp.cap, fp.cap, qn, me, 32, bits_for(n - 1), sk + q0 * me, si + q0 * me, st,
+                    cnt);
+        w.mark(st, 3);
+      }
       break;
     }
     case OVB_INDEX_KIND_MULTIBUCKET: {
@@ -170,6 +259,7 @@ uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint6
       uint64_t* qb = (uint64_t*)w.qbits.ensure(nq * nb * qpb * 8);
       launch_multibucket_query(d_q, nq, s1.dim, s1.bits, qb, st);
       w.mark(st, 1);
+      w.mark(st, 6);  // no sampling stage
       const float* wts = d_weights;
       if (!wts) {  // diagonal weights (src/multi_bucket.rs:157-164)
         std::vector<float> diag(nb * nb, 0.0f);

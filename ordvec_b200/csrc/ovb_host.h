@@ -96,7 +96,10 @@ struct Workspace {
   cudaStream_t stream = nullptr;
   DevBuf q_raw, q_unit, qbits, lut, bias, invq, keys, sel_keys, sel_ids, off, keys2, out_keys,
       out_ids, scores, ids, scratch, stage, weights, flag;
-  HostBuf pinned;
+  // FastScan threshold filter: sample key matrix, per-query thresholds,
+  // kept (key, id) rows, their counts and the failure flag
+  DevBuf smp_keys, thr_keys, thr_ids, f_keys, f_ids, f_cnt, f_flag;
+  HostBuf pinned, f_flag_host;
   // error word of the tensor-core kernels (zeroed once; checked by host APIs)
   DevBuf tc_err;
   bool tc_used = false;
@@ -108,8 +111,10 @@ struct Workspace {
     tc_used = true;
     return tc_err.as<uint32_t>();
   }
-  // stage markers for ovb_two_stage_profile (recorded only while prof is set)
-  cudaEvent_t prof_ev[6] = {};
+  // stage markers for ovb_two_stage_profile (recorded only while prof is set):
+  // 0 start, 1 query prep, 6 candidate threshold, 2 scan, 3 select, 4 rerank,
+  // 5 final select
+  cudaEvent_t prof_ev[7] = {};
   bool prof = false;
   void mark(cudaStream_t st, int i) {
     if (prof) OVB_CUDA(cudaEventRecord(prof_ev[i], st));

@@ -22,6 +22,7 @@ struct SelectArgs {
   uint32_t id_bits;   // significant bits of id32
   uint32_t* out_keys;
   uint32_t* out_ids;
+  const uint32_t* row_len;  // optional: row r holds min(row_len[r], n) entries at r*ld
 };
 size_t select_rows_scratch_elems(uint64_t rows, uint32_t k);
 void launch_select_rows(const SelectArgs& a, uint64_t rows, uint64_t* scratch,
@@ -60,10 +61,24 @@ void launch_fastscan_scan(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad,
                           float inv_norm, uint64_t nq, uint32_t* keys, uint64_t ld,
                           cudaStream_t stream);
 // Tensor-core form (scan_fastscan_tc.cu): same keys, bit for bit; *err (device
-// u32) gets bit 0 set if a bounded wait timed out.
+// u32) gets bit 0 set if a bounded wait timed out.  block_stride > 1 scores
+// only every block_stride-th 32-doc block; keys[q][u] then holds the u-th
+// sampled doc (fastscan_tc_sample_docs columns).
 void launch_fastscan_scan_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad, const uint8_t* lut,
                              const float* bias_sum, const float* inv_q, float inv_norm, uint64_t nq,
-                             uint32_t* keys, uint64_t ld, uint32_t* err, cudaStream_t stream);
+                             uint32_t block_stride, uint32_t* keys, uint64_t ld, uint32_t* err,
+                             cudaStream_t stream);
+uint64_t fastscan_tc_sample_docs(uint64_t n, uint32_t block_stride);
+// Threshold filter: appends (key32, doc) with key32 <= thr[q * thr_stride] to
+// row q of f_keys / f_ids (capacity cap); cnt[q] (zeroed by the caller) counts
+// every qualifying doc.
+void launch_fastscan_filter_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad, const uint8_t* lut,
+                               const float* bias_sum, const float* inv_q, float inv_norm, uint64_t nq,
+                               const uint32_t* thr, uint64_t thr_stride, uint32_t* cnt, uint32_t cap,
+                               uint32_t* f_keys, uint32_t* f_ids, uint32_t* err, cudaStream_t stream);
+// *flag |= 1 when some cnt[q] < need or > cap.
+void launch_filter_check(const uint32_t* cnt, uint64_t nq, uint32_t need, uint32_t cap, uint32_t* flag,
+                         cudaStream_t stream);
 void launch_fastscan_relayout(const uint8_t* ref_blocks, uint64_t n, uint32_t pairs,
                               uint32_t pairs_pad, uint8_t* dev_blocks, cudaStream_t stream);
 

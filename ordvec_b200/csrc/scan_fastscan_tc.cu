@@ -4,21 +4,35 @@
 //   acc[doc][q] = sum_p LUT_q[p][nib_p(doc)] = sum_k onehot(doc)[k] * LUT_q[k],
 //   k = 16 p + nibble  (K = pairs_pad * 16 = 8192 at dim 1024)
 //
-// A (M = 128 docs x K) is the one-hot expansion of the nibble codes, built in
-// shared memory by the CTA's threads; B (N = up to 256 queries x K) is the u8
-// LUT matrix, loaded by TMA; D (128 x N, s32) accumulates in tensor memory with
-// tcgen05.mma kind::i8 (u8 x u8).  Both operands use the K-major 128-byte
-// swizzled layout: row r of a 128-byte K-block at (r/8)*1024 + (r%8)*128, its
-// 16-byte chunk c at ((c ^ r%8) * 16).  The sum is exact, so the scores
+// A (docs x K) is the one-hot expansion of the nibble codes, built in shared
+// memory by the CTA's threads; B (N = up to 256 queries x K) is the u8 LUT
+// matrix, loaded by TMA; D (s32) accumulates in tensor memory with
+// tcgen05.mma kind::i8 (u8 x u8).  A CTA owns 256 docs as two M=128
+// accumulators (TMEM columns [0, N) and [256, 256 + N)), so every LUT byte it
+// loads feeds 256 docs.  Both operands use the K-major 128-byte swizzled
+// layout: row r of a 128-byte K-block at (r/8)*1024 + (r%8)*128, its 16-byte
+// chunk c at ((c ^ r%8) * 16).  The sum is exact, so the scores
 //   (bias + (acc as f32) * inv_q) * inv_norm
 // equal the CUDA-core kernel's (and the reference's) bit for bit.
 //
-// Pipeline: STAGES smem stages of (A 16 KiB + B up to 32 KiB); per K-block all
-// threads expand A while thread 0 issues the B TMA, then thread 0 issues four
-// K=32 MMAs and commits them to the stage's mbarrier, which the threads wait
-// on before reusing the stage.  Every wait is bounded: on timeout the kernel
-// records an error bit, stops issuing work, waits (bounded) for what it issued,
-// frees its tensor memory and returns.
+// Warp roles (576 threads):
+//   warp 0, lane 0   TMA producer: LUT K-block -> stage s   (waits empty[s])
+//   warp 1, lane 0   MMA issuer: 8 MMAs per K-block, commit -> empty[s]
+//   warps 2..17      A builders, two threads per doc row, four 16-byte chunks
+//                    each (wait empty[s], one arrive per warp on full_a[s]);
+//                    afterwards the epilogue (TMEM -> keys)
+// STAGES smem stages of (A 32 KiB + B 32 KiB) let the producer and builders run
+// ahead of the tensor core.  Every wait is bounded: on timeout the kernel sets
+// bit 0 of *err, stops issuing work, waits (bounded) for the copies and MMAs it
+// issued, frees its tensor memory and returns.
+//
+// Epilogue modes:
+//   dense   keys[q][u] = key32 for every logical doc u (the key matrix)
+//   filter  only keys <= thr[q] are appended to row q of a capacity-`cap`
+//           buffer (key, doc id) through an atomic counter; cnt[q] ends as the
+//           number of qualifying docs even when it exceeds `cap`.
+// Doc sampling: logical 32-doc block ub reads physical block ub * block_stride,
+// so a stride > 1 scores an evenly spread sample of the index.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -29,25 +43,62 @@ namespace ovb {
 
 namespace {
 
-constexpr int kTcThreads = 128;
-constexpr int kTcM = 128;
+constexpr int kTcThreads = 576;
+constexpr int kTcBuilders = 512;  // warps 2..17
+constexpr int kTcM = 256;         // docs per CTA (two M=128 accumulators)
 constexpr int kTcMaxN = 256;
 constexpr int kTcKBytes = 128;  // 8 pairs x 16 one-hot bytes per K-block
 constexpr int kTcStages = 3;
-constexpr uint32_t kAStage = kTcM * kTcKBytes;       // 16 KiB
-constexpr uint32_t kBStage = kTcMaxN * kTcKBytes;    // 32 KiB
-constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kAHalf = 128 * kTcKBytes;        // 16 KiB
+constexpr uint32_t kAStage = kTcM * kTcKBytes;      // 32 KiB
+constexpr uint32_t kBStage = kTcMaxN * kTcKBytes;   // 32 KiB
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kAcc1Col = 256;
 constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s
+constexpr uint32_t kSuspendNs = 100000;       // try_wait sleep hint (0.1 ms)
+// filter epilogue list (key, q | slot << 8 | row << 16) in the dead A stages
+constexpr uint32_t kListCap = kTcStages * kAStage / 8;
 
 struct TcSmem {
   uint8_t a[kTcStages][kAStage];
   uint8_t b[kTcStages][kBStage];
   float bias[kTcMaxN];
   float invq[kTcMaxN];
-  uint64_t mbar_tma[kTcStages];
-  uint64_t mbar_mma[kTcStages];
+  uint32_t thr[kTcMaxN];
+  uint64_t full_a[kTcStages];
+  uint64_t full_b[kTcStages];
+  uint64_t empty[kTcStages];
+  uint64_t acc_full;
+  uint32_t cnt[kTcMaxN];   // filter: kept docs per query in this tile
+  uint32_t base[kTcMaxN];  // filter: the tile's first slot in each query row
+  uint32_t list_n;
+  uint32_t epi_ok;
   uint32_t tmem;
   uint32_t abort;
+};
+
+struct TcArgs {
+  const uint8_t* blocks;
+  uint64_t n;
+  uint32_t pairs_pad;
+  uint32_t block_stride;
+  const float* bias;
+  const float* invq;
+  float inv_norm;
+  uint64_t nq;
+  uint32_t nt;
+  // dense output (keys != null)
+  uint32_t* keys;
+  uint64_t ld;
+  // filter output
+  const uint32_t* thr;
+  uint64_t thr_stride;
+  uint32_t* cnt;
+  uint32_t cap;
+  uint32_t* f_keys;
+  uint32_t* f_ids;
+  uint32_t* err;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -63,21 +114,68 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
-// Bounded parity wait; returns false on timeout.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// One potentially blocking poll: the thread sleeps until the phase completes
+// or kSuspendNs pass, so waiting warps do not spin on the issue slots.
+__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(addr), "r"(parity), "n"(kSuspendNs)
+      : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ uint32_t atom_add_shared(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.shared::cta.add.u32 %0, [%1], %2;" : "=r"(old) : "r"(smem_u32(p)), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded parity wait: at most kWaitLimit polls and about kWaitNs of wall
+// time; returns false on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   const uint32_t addr = smem_u32(bar);
+  if (mbar_try(addr, parity)) return true;
+  const uint64_t t0 = global_ns();
   for (uint32_t it = 0; it < kWaitLimit; it++) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (done) return true;
+    if (mbar_try(addr, parity)) return true;
+    if (global_ns() - t0 > kWaitNs) return false;
   }
   return false;
+}
+
+// named barrier 1 over the builder / epilogue threads (warps 2..17)
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kTcBuilders) : "memory"); }
+
+// shl.b32 clamps shift amounts >= 32 to 32 (result 0); a "negative" amount
+// wraps to a large unsigned one, so shl1(8 * nib - 32 * i) is the word i of the
+// 16-byte one-hot row of nibble nib.
+__device__ __forceinline__ uint32_t shl1(uint32_t amount) {
+  uint32_t r;
+  asm("shl.b32 %0, %1, %2;" : "=r"(r) : "r"(1u), "r"(amount));
+  return r;
+}
+
+__device__ __forceinline__ void raise_abort(TcSmem& S, uint32_t* err) {
+  atomicExch(&S.abort, 1u);
+  atomicOr(err, 1u);
+}
+
+__device__ __forceinline__ bool aborted(const TcSmem& S) {
+  return *reinterpret_cast<const volatile uint32_t*>(&S.abort) != 0;
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
@@ -124,17 +222,25 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ uint4 load_codes(const uint8_t* p) {
+  uint4 v;
+  asm volatile("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
+}
+
 __global__ void __launch_bounds__(kTcThreads, 1)
-    fastscan_tc_kernel(const uint8_t* __restrict__ blocks, uint64_t n, uint32_t pairs_pad,
-                       const __grid_constant__ CUtensorMap lut_map, const float* __restrict__ bias,
-                       const float* __restrict__ invq, float inv_norm, uint64_t nq, uint32_t nt,
-                       uint32_t* __restrict__ keys, uint64_t ld, uint32_t* __restrict__ err) {
+    fastscan_tc_kernel(const __grid_constant__ CUtensorMap lut_map, const TcArgs a) {
   extern __shared__ uint8_t smem_raw[];
   TcSmem& S = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  const int t = threadIdx.x, warp = t >> 5;
-  const uint64_t doc0 = (uint64_t)blockIdx.x * kTcM;
-  const uint64_t q0 = (uint64_t)blockIdx.y * nt;
-  const uint32_t nqt = (uint32_t)((nq - q0) < nt ? (nq - q0) : nt);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const uint64_t q0 = (uint64_t)blockIdx.y * a.nt;
+  const uint32_t nt = a.nt;
+  const uint32_t nqt = (uint32_t)((a.nq - q0) < nt ? (a.nq - q0) : nt);
+  const uint64_t n_blocks = (a.n + 31) / 32;
+  const uint32_t n_kb = a.pairs_pad / 8;
+  const bool dense = a.keys != nullptr;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
@@ -142,103 +248,214 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  if (t == 0) {
+  if (t == 32) {
     for (int s = 0; s < kTcStages; s++) {
-      mbar_init(&S.mbar_tma[s], 1);
-      mbar_init(&S.mbar_mma[s], 1);
+      mbar_init(&S.full_a[s], kTcBuilders / 32);  // one arrive per builder warp
+      mbar_init(&S.full_b[s], 1);
+      mbar_init(&S.empty[s], 1);
     }
+    mbar_init(&S.acc_full, 1);
     S.abort = 0;
+    S.list_n = 0;
+    S.epi_ok = 1;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (uint32_t i = t; i < nt; i += kTcThreads) {
-    S.bias[i] = i < nqt ? bias[q0 + i] : 0.0f;
-    S.invq[i] = i < nqt ? invq[q0 + i] : 0.0f;
+    const bool v = i < nqt;
+    S.bias[i] = v ? a.bias[q0 + i] : 0.0f;
+    S.invq[i] = v ? a.invq[q0 + i] : 0.0f;
+    S.thr[i] = (v && !dense) ? a.thr[(q0 + i) * a.thr_stride] : 0u;
+    S.cnt[i] = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = S.tmem;
 
-  // instruction descriptor: D s32, A/B u8, K-major, N = nt, M = 128
-  const uint32_t idesc = (2u << 4) | ((nt >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
-  const uint32_t b_bytes = nt * kTcKBytes;
-
-  const uint32_t r = t;  // A row = doc within the tile
-  const uint64_t doc = doc0 + r;
-  const uint64_t n_blocks = (n + 31) / 32;
-  const uint64_t blk = doc / 32;
-  const uint32_t dl = (uint32_t)(doc % 32);
-  const bool row_valid = blk < n_blocks;
-  const uint8_t* row_codes = blocks + blk * (uint64_t)pairs_pad * 16 + (uint64_t)dl * 16;
-  const uint32_t n_kb = pairs_pad / 8;
-  uint4 chunk = make_uint4(0, 0, 0, 0);
-  uint32_t issued = 0;          // K-blocks whose MMAs were committed (thread 0)
-  int pending_tma = -1;         // stage of a TMA whose wait timed out (thread 0)
-  uint32_t pending_parity = 0;
-
-  for (uint32_t kb = 0; kb < n_kb; kb++) {
-    const uint32_t s = kb % kTcStages, it = kb / kTcStages;
-    if (kb >= kTcStages && !mbar_wait(&S.mbar_mma[s], (it - 1) & 1)) atomicOr(&S.abort, 1u);
-    __syncthreads();
-    if (S.abort) break;
-    if (t == 0) {
-      mbar_expect_tx(&S.mbar_tma[s], b_bytes);
-      tma_load_2d(S.b[s], &lut_map, (int)(kb * kTcKBytes), (int)q0, &S.mbar_tma[s]);
-    }
-    if ((kb & 3) == 0)
-      chunk = row_valid ? *reinterpret_cast<const uint4*>(row_codes + (uint64_t)(kb >> 2) * 512)
-                        : make_uint4(0, 0, 0, 0);
-    const uint32_t w = (kb & 3) == 0 ? chunk.x : (kb & 3) == 1 ? chunk.y : (kb & 3) == 2 ? chunk.z : chunk.w;
-    uint8_t* arow = S.a[s] + (r >> 3) * 1024 + (r & 7) * 128;
-#pragma unroll
-    for (uint32_t c = 0; c < 8; c++) {
-      const uint32_t nib = (w >> (4 * c)) & 15;
-      const uint32_t one = 1u << (8 * (nib & 3)), sel = nib >> 2;
-      uint4 v = make_uint4(sel == 0 ? one : 0, sel == 1 ? one : 0, sel == 2 ? one : 0, sel == 3 ? one : 0);
-      *reinterpret_cast<uint4*>(arow + ((c ^ (r & 7)) << 4)) = v;
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (t == 0) {
-      if (!mbar_wait(&S.mbar_tma[s], it & 1)) {
-        atomicOr(&S.abort, 1u);
-        pending_tma = (int)s;
-        pending_parity = it & 1;
-      } else {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t a_base = smem_u32(S.a[s]), b_base = smem_u32(S.b[s]);
-#pragma unroll
-        for (uint32_t j = 0; j < 4; j++)
-          mma_i8(tmem, sw128_desc(a_base + 32 * j), sw128_desc(b_base + 32 * j), idesc, (kb | j) != 0);
-        mma_commit(&S.mbar_mma[s]);
+  if (warp == 0) {
+    // ---- TMA producer --------------------------------------------------------
+    if (lane == 0) {
+      const uint32_t b_bytes = nt * kTcKBytes;
+      uint32_t issued = 0;
+      for (uint32_t kb = 0; kb < n_kb; kb++) {
+        const uint32_t s = kb % kTcStages, it = kb / kTcStages;
+        if (aborted(S)) break;
+        if (kb >= kTcStages && !mbar_wait(&S.empty[s], (it - 1) & 1)) {
+          raise_abort(S, a.err);
+          break;
+        }
+        mbar_expect_tx(&S.full_b[s], b_bytes);
+        tma_load_2d(S.b[s], &lut_map, (int)(kb * kTcKBytes), (int)q0, &S.full_b[s]);
         issued = kb + 1;
       }
+      // every issued copy lands before the CTA exits (the latest phase of each
+      // stage covers the earlier ones)
+      for (uint32_t kb = issued > kTcStages ? issued - kTcStages : 0; kb < issued; kb++)
+        mbar_wait(&S.full_b[kb % kTcStages], (kb / kTcStages) & 1);
     }
-  }
-  // drain: a TMA whose wait timed out must land before the CTA exits, and the
-  // last committed MMA group (which covers all earlier ones) must finish
-  if (t == 0 && pending_tma >= 0) mbar_wait(&S.mbar_tma[pending_tma], pending_parity);
-  __shared__ uint32_t s_issued;
-  if (t == 0) s_issued = issued;
-  __syncthreads();
-  const uint32_t last = s_issued;
-  bool ok = last == n_kb;
-  if (last > 0 && !mbar_wait(&S.mbar_mma[(last - 1) % kTcStages], ((last - 1) / kTcStages) & 1)) ok = false;
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (!ok || S.abort) {
-    if (t == 0) atomicOr(err, 1u);
-  } else {
-    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-    for (uint32_t cb = 0; cb < nt; cb += 32) {
-      uint32_t v[32];
-      tmem_ld32(tmem + lane_base + cb, v);
-      if (doc < n) {
+  } else if (warp == 1) {
+    // ---- MMA issuer ----------------------------------------------------------
+    if (lane == 0) {
+      // D s32, A/B u8, both K-major, N = nt, M = 128
+      const uint32_t idesc = (2u << 4) | ((nt >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+      uint32_t done = 0;
+      for (uint32_t kb = 0; kb < n_kb; kb++) {
+        const uint32_t s = kb % kTcStages, it = kb / kTcStages;
+        if (aborted(S)) break;
+        if (!mbar_wait(&S.full_b[s], it & 1) || !mbar_wait(&S.full_a[s], it & 1)) {
+          raise_abort(S, a.err);
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a0 = smem_u32(S.a[s]), b0 = smem_u32(S.b[s]);
 #pragma unroll
-        for (uint32_t j = 0; j < 32; j++) {
-          const uint32_t q = cb + j;
-          if (q < nqt) {
-            const float sc = __fmul_rn(__fadd_rn(S.bias[q], __fmul_rn(__uint2float_rn(v[j]), S.invq[q])), inv_norm);
-            keys[(q0 + q) * ld + doc] = desc_key(sc);
+        for (uint32_t j = 0; j < 4; j++) {
+          const uint64_t bd = sw128_desc(b0 + 32 * j);
+          const uint32_t acc = (kb | j) != 0;
+          mma_i8(tmem, sw128_desc(a0 + 32 * j), bd, idesc, acc);
+          mma_i8(tmem + kAcc1Col, sw128_desc(a0 + kAHalf + 32 * j), bd, idesc, acc);
+        }
+        mma_commit(&S.empty[s]);
+        done = kb + 1;
+      }
+      // the issuer itself waits (bounded) for its last commit, which covers
+      // every earlier MMA, so no MMA is in flight when the CTA frees TMEM
+      if (done == n_kb && !aborted(S)) {
+        mma_commit(&S.acc_full);
+        mbar_wait(&S.acc_full, 0);
+      } else if (done > 0) {
+        mbar_wait(&S.empty[(done - 1) % kTcStages], ((done - 1) / kTcStages) & 1);
+      }
+    }
+  } else {
+    // ---- A builders: row r = doc (tile-local), chunks 4*hc .. 4*hc+3 ----------
+    const uint32_t bt = (uint32_t)t - 64;
+    const uint32_t r = bt & 255, hc = bt >> 8;
+    {
+      const uint64_t pb = ((uint64_t)blockIdx.x * 8 + (r >> 5)) * a.block_stride;
+      const bool row_valid = pb < n_blocks;
+      const uint8_t* row_codes = a.blocks + pb * (uint64_t)a.pairs_pad * 16 + (uint64_t)(r & 31) * 16;
+      const uint32_t a_off = (r >> 7) * kAHalf + ((r & 127) >> 3) * 1024 + (r & 7) * 128;
+      const uint32_t swz = r & 7;
+      uint4 chunk = make_uint4(0, 0, 0, 0);
+      uint4 next = row_valid ? load_codes(row_codes) : make_uint4(0, 0, 0, 0);
+      for (uint32_t kb = 0; kb < n_kb; kb++) {
+        const uint32_t s = kb % kTcStages, it = kb / kTcStages;
+        if ((kb & 3) == 0) {
+          chunk = next;
+          const uint32_t g = (kb >> 2) + 1;  // next 32-pair group
+          if (row_valid && g * 4 < n_kb) next = load_codes(row_codes + (uint64_t)g * 512);
+        }
+        // warp-uniform control flow: lane 0 waits for the stage, the warp
+        // follows its verdict
+        if (__any_sync(0xFFFFFFFFu, aborted(S))) break;
+        if (kb >= kTcStages) {
+          bool ok = true;
+          if (lane == 0) ok = mbar_wait(&S.empty[s], (it - 1) & 1);
+          ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
+          if (!ok) {
+            if (lane == 0) raise_abort(S, a.err);
+            break;
+          }
+          __syncwarp();
+        }
+        const uint32_t w4 = (kb & 3) == 0 ? chunk.x : (kb & 3) == 1 ? chunk.y : (kb & 3) == 2 ? chunk.z : chunk.w;
+        const uint32_t w = w4 >> (16 * hc);  // this thread's four nibbles
+        uint8_t* arow = S.a[s] + a_off;
+#pragma unroll
+        for (uint32_t c = 0; c < 4; c++) {
+          const uint32_t sh = c == 0 ? (w << 3) & 0x78u : (w >> (4 * c - 3)) & 0x78u;  // 8 * nibble
+          const uint4 v = make_uint4(shl1(sh), shl1(sh - 32), shl1(sh - 64), shl1(sh - 96));
+          *reinterpret_cast<uint4*>(arow + (((4 * hc + c) ^ swz) << 4)) = v;
+        }
+        // each lane makes its rows visible to the tensor core's (async) proxy;
+        // the warp barrier orders all lanes before lane 0's release-arrive
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&S.full_a[s]);
+      }
+    }
+
+    // ---- epilogue: TMEM lane quarter (warp % 4), accumulator half ------------
+    bool ready = false;
+    if (lane == 0) {
+      const uint32_t addr = smem_u32(&S.acc_full);
+      const uint64_t t0 = global_ns();
+      for (uint32_t it = 0; it < kWaitLimit && !aborted(S); it++) {
+        if (mbar_try(addr, 0)) {
+          ready = true;
+          break;
+        }
+        if (global_ns() - t0 > kWaitNs) break;
+      }
+      if (!ready && !aborted(S)) raise_abort(S, a.err);
+    }
+    ready = __shfl_sync(0xFFFFFFFFu, ready, 0);
+    __syncwarp();
+    // one decision for all epilogue threads (they share named barrier 1)
+    if (!ready || aborted(S)) atomicExch(&S.epi_ok, 0u);
+    epi_bar();
+    ready = *reinterpret_cast<volatile uint32_t*>(&S.epi_ok) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ready) {
+      // warps 2..17: TMEM lane quarter warp % 4 (hardware rule), accumulator
+      // half h, and every other 32-column chunk starting at c0
+      const uint32_t eg = (uint32_t)(warp - 2) >> 2;
+      const uint32_t h = eg & 1, c0 = (eg >> 1) * 32, lq = (uint32_t)warp & 3;
+      const uint32_t row = h * 128 + lq * 32 + lane;
+      const uint64_t pb = ((uint64_t)blockIdx.x * 8 + (row >> 5)) * a.block_stride;
+      const uint64_t doc = pb * 32 + lane;
+      const uint64_t u = (uint64_t)blockIdx.x * kTcM + row;
+      const bool valid = pb < n_blocks && doc < a.n;
+      const uint32_t taddr = tmem + ((lq * 32) << 16) + h * kAcc1Col;
+      // filter list: the A stages are dead once acc_full has fired
+      uint2* list = reinterpret_cast<uint2*>(&S.a[0][0]);
+      for (uint32_t cb = c0; cb < nt; cb += 64) {
+        uint32_t v[32];
+        __syncwarp();
+        tmem_ld32(taddr + cb, v);
+        if (valid) {
+#pragma unroll
+          for (uint32_t j = 0; j < 32; j++) {
+            const uint32_t q = cb + j;
+            if (q < nqt) {
+              const float sc =
+                  __fmul_rn(__fadd_rn(S.bias[q], __fmul_rn(__uint2float_rn(v[j]), S.invq[q])), a.inv_norm);
+              const uint32_t key = desc_key(sc);
+              if (dense) {
+                a.keys[(q0 + q) * a.ld + u] = key;
+              } else if (key <= S.thr[q]) {
+                const uint32_t e = atom_add_shared(&S.list_n, 1u);
+                if (e < kListCap) {
+                  const uint32_t li = atom_add_shared(&S.cnt[q], 1u);  // < 256: one slot per row
+                  list[e] = make_uint2(key, q | (li << 8) | (row << 16));
+                } else {  // list full: claim a global slot directly
+                  const uint32_t pos = atomicAdd(&a.cnt[q0 + q], 1u);
+                  if (pos < a.cap) {
+                    a.f_keys[(q0 + q) * a.cap + pos] = key;
+                    a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)doc;
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+      if (!dense) {
+        // one global atomic per query per tile, then the scattered writes
+        epi_bar();
+        const uint32_t i = (uint32_t)t - 64;
+        if (i < nqt && S.cnt[i]) S.base[i] = atomicAdd(&a.cnt[q0 + i], S.cnt[i]);
+        epi_bar();
+        const uint32_t total = S.list_n < kListCap ? S.list_n : kListCap;
+        for (uint32_t e = i; e < total; e += kTcBuilders) {
+          const uint2 en = list[e];
+          const uint32_t q = en.y & 255, li = (en.y >> 8) & 255, rw = en.y >> 16;
+          const uint32_t pos = S.base[q] + li;
+          if (pos < a.cap) {
+            a.f_keys[(q0 + q) * a.cap + pos] = en.x;
+            const uint64_t rpb = ((uint64_t)blockIdx.x * 8 + (rw >> 5)) * a.block_stride;
+            a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw & 31));
           }
         }
       }
@@ -248,6 +465,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+__global__ void filter_check_kernel(const uint32_t* __restrict__ cnt, uint64_t nq, uint32_t need, uint32_t cap,
+                                    uint32_t* __restrict__ flag) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nq) {
+    const uint32_t c = cnt[i];
+    if (c < need || c > cap) atomicOr(flag, 1u);
+  }
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -262,35 +488,89 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-}  // namespace
-
-size_t fastscan_tc_smem_bytes() { return sizeof(TcSmem) + 1024; }
-
-void launch_fastscan_scan_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad, const uint8_t* lut,
-                             const float* bias_sum, const float* inv_q, float inv_norm, uint64_t nq,
-                             uint32_t* keys, uint64_t ld, uint32_t* err, cudaStream_t stream) {
-  if (!n || !nq) return;
-  const uint64_t k_bytes = (uint64_t)pairs_pad * 16;
+void launch_tc(TcArgs a, const uint8_t* lut, cudaStream_t stream) {
+  if (!a.n || !a.nq) return;
+  const uint64_t k_bytes = (uint64_t)a.pairs_pad * 16;
   // N per tile: a multiple of 16 in [16, 256]
-  uint32_t nt = nq >= kTcMaxN ? kTcMaxN : (uint32_t)((nq + 15) / 16 * 16);
+  a.nt = a.nq >= kTcMaxN ? kTcMaxN : (uint32_t)((a.nq + 15) / 16 * 16);
   CUtensorMap map;
-  cuuint64_t gdim[2] = {(cuuint64_t)k_bytes, (cuuint64_t)nq};
+  cuuint64_t gdim[2] = {(cuuint64_t)k_bytes, (cuuint64_t)a.nq};
   cuuint64_t gstride[1] = {(cuuint64_t)k_bytes};
-  cuuint32_t box[2] = {(cuuint32_t)kTcKBytes, (cuuint32_t)nt};
+  cuuint32_t box[2] = {(cuuint32_t)kTcKBytes, (cuuint32_t)a.nt};
   cuuint32_t estride[2] = {1, 1};
   CUresult rc = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)lut, gdim, gstride, box, estride,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (rc != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed for the FastScan LUT matrix");
-  const size_t smem = fastscan_tc_smem_bytes();
+  const size_t smem = sizeof(TcSmem) + 1024;
   OVB_CUDA(cudaFuncSetAttribute(fastscan_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const uint64_t doc_tiles = (n + kTcM - 1) / kTcM;
-  const uint64_t q_tiles = (nq + nt - 1) / nt;
+  const uint64_t n_blocks = (a.n + 31) / 32;
+  const uint64_t logical_blocks = (n_blocks + a.block_stride - 1) / a.block_stride;
+  const uint64_t doc_tiles = (logical_blocks + 7) / 8;
+  const uint64_t q_tiles = (a.nq + a.nt - 1) / a.nt;
   if (q_tiles > 65535 || doc_tiles > 0x7FFFFFFF)
     throw std::invalid_argument("FastScan tensor-core scan: grid too large; split the query batch");
   dim3 grid((unsigned)doc_tiles, (unsigned)q_tiles);
-  fastscan_tc_kernel<<<grid, kTcThreads, smem, stream>>>(blocks, n, pairs_pad, map, bias_sum, inv_q, inv_norm, nq,
-                                                         nt, keys, ld, err);
+  fastscan_tc_kernel<<<grid, kTcThreads, smem, stream>>>(map, a);
+  launched();
+}
+
+}  // namespace
+
+uint64_t fastscan_tc_sample_docs(uint64_t n, uint32_t block_stride) {
+  const uint64_t n_blocks = (n + 31) / 32;
+  if (!n_blocks) return 0;
+  const uint64_t sampled = (n_blocks + block_stride - 1) / block_stride;
+  const uint64_t last = (sampled - 1) * block_stride;  // the only block that can be partial
+  return (sampled - 1) * 32 + (last == n_blocks - 1 ? n - last * 32 : 32);
+}
+
+void launch_fastscan_scan_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad, const uint8_t* lut,
+                             const float* bias_sum, const float* inv_q, float inv_norm, uint64_t nq,
+                             uint32_t block_stride, uint32_t* keys, uint64_t ld, uint32_t* err,
+                             cudaStream_t stream) {
+  TcArgs a{};
+  a.blocks = blocks;
+  a.n = n;
+  a.pairs_pad = pairs_pad;
+  a.block_stride = block_stride ? block_stride : 1;
+  a.bias = bias_sum;
+  a.invq = inv_q;
+  a.inv_norm = inv_norm;
+  a.nq = nq;
+  a.keys = keys;
+  a.ld = ld;
+  a.err = err;
+  launch_tc(a, lut, stream);
+}
+
+void launch_fastscan_filter_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad, const uint8_t* lut,
+                               const float* bias_sum, const float* inv_q, float inv_norm, uint64_t nq,
+                               const uint32_t* thr, uint64_t thr_stride, uint32_t* cnt, uint32_t cap,
+                               uint32_t* f_keys, uint32_t* f_ids, uint32_t* err, cudaStream_t stream) {
+  TcArgs a{};
+  a.blocks = blocks;
+  a.n = n;
+  a.pairs_pad = pairs_pad;
+  a.block_stride = 1;
+  a.bias = bias_sum;
+  a.invq = inv_q;
+  a.inv_norm = inv_norm;
+  a.nq = nq;
+  a.thr = thr;
+  a.thr_stride = thr_stride;
+  a.cnt = cnt;
+  a.cap = cap;
+  a.f_keys = f_keys;
+  a.f_ids = f_ids;
+  a.err = err;
+  launch_tc(a, lut, stream);
+}
+
+void launch_filter_check(const uint32_t* cnt, uint64_t nq, uint32_t need, uint32_t cap, uint32_t* flag,
+                         cudaStream_t stream) {
+  if (!nq) return;
+  filter_check_kernel<<<(unsigned)((nq + 255) / 256), 256, 0, stream>>>(cnt, nq, need, cap, flag);
   launched();
 }
 

@@ -70,6 +70,7 @@ __global__ void __launch_bounds__(kSelThreads)
   } else {
     start = row * a.ld;
     n = a.n;
+    if (a.row_len && a.row_len[row] < n) n = a.row_len[row];
   }
   const uint32_t* keys = a.keys + start;
   const uint32_t* ids = a.ids ? a.ids + start : nullptr;
@@ -348,7 +349,7 @@ void launch_select_rows(const SelectArgs& a, uint64_t rows, uint64_t* scratch,
                         cudaStream_t stream) {
   if (rows == 0) return;
   // few long rows: one 8-CTA cluster per row
-  if (!a.row_off && a.k <= kClusterCap && a.n >= 32768 && rows * kClusterCtas <= 2 * 148) {
+  if (!a.row_off && !a.row_len && a.k <= kClusterCap && a.n >= 32768 && rows * kClusterCtas <= 2 * 148) {
     select_rows_cluster_kernel<<<(unsigned)(rows * kClusterCtas), kSelThreads, 0, stream>>>(a);
     launched();
     return;

@@ -373,6 +373,80 @@ def test_fastscan_tensor_core_path_is_bit_exact(orc, monkeypatch, dim, n, nq):
     assert np.array_equal(tc.scores.reshape(nq, k)[:4].view(np.uint32), s_ref.view(np.uint32))
 
 
+def _fastscan_modes(monkeypatch, fs, queries, k, **env):
+    """Search once per environment setting; returns the results in order."""
+    out = []
+    for name, settings in env.items():
+        for var in ("OVB_FASTSCAN_TC", "OVB_FASTSCAN_FILTER", "OVB_FASTSCAN_SAMPLE_MULT"):
+            monkeypatch.delenv(var, raising=False)
+        for var, val in settings.items():
+            monkeypatch.setenv(var, val)
+        out.append(fs.search(queries, k))
+    for var in ("OVB_FASTSCAN_TC", "OVB_FASTSCAN_FILTER", "OVB_FASTSCAN_SAMPLE_MULT"):
+        monkeypatch.delenv(var, raising=False)
+    return out
+
+
+def _same(a, b):
+    assert np.array_equal(a.indices, b.indices)
+    assert np.array_equal(a.scores.view(np.uint32), b.scores.view(np.uint32))
+
+
+@pytest.mark.parametrize(
+    "dim,n,nq,k,mult",
+    [
+        (256, 40_000, 70, 200, None),    # sample stride 4
+        (256, 39_950, 40, 64, None),     # last (partial) block is sampled
+        (100, 70_001, 300, 333, None),   # two query tiles, odd pair count
+        (256, 40_000, 70, 200, "0.02"),  # threshold too tight -> dense redo
+        (256, 40_000, 70, 200, "1e6"),   # threshold keeps all -> over capacity -> dense redo
+    ],
+)
+def test_fastscan_threshold_filter_is_exact(orc, monkeypatch, dim, n, nq, k, mult):
+    """Sample-threshold filter (TC scan keeping only keys <= a per-query
+    threshold) returns exactly the key-matrix result, ids and score bits, and
+    its fallback does too."""
+    docs = ob.synth_docs(29, n, dim)
+    queries, _ = ob.synth_queries(29, n, nq, dim)
+    fs = ob.RankQuantFastscan(dim)
+    fs.add(docs)
+    filt = {"OVB_FASTSCAN_TC": "1", "OVB_FASTSCAN_FILTER": "1"}
+    if mult:
+        filt["OVB_FASTSCAN_SAMPLE_MULT"] = mult
+    f, d, c = _fastscan_modes(
+        monkeypatch, fs, queries, k,
+        filt=filt,
+        dense={"OVB_FASTSCAN_TC": "1", "OVB_FASTSCAN_FILTER": "0"},
+        cuda_core={"OVB_FASTSCAN_TC": "0"},
+    )
+    _same(f, d)
+    _same(f, c)
+    s_ref, i_ref = orc.fastscan_search(orc.fastscan_pack(docs, dim), n, dim, queries[:3], k)
+    assert np.array_equal(f.indices.reshape(nq, k)[:3], i_ref)
+    assert np.array_equal(f.scores.reshape(nq, k)[:3].view(np.uint32), s_ref.view(np.uint32))
+
+
+def test_fastscan_threshold_filter_heavy_ties(orc, monkeypatch):
+    """500 distinct rows tiled 80x: the top-k is decided by doc id among equal
+    keys; the filter path keeps every tie and orders them like the oracle."""
+    dim, base, reps, nq, k = 128, 500, 80, 48, 150
+    distinct = ob.synth_docs(37, base, dim)
+    docs = np.tile(distinct, (reps, 1))
+    n = base * reps
+    queries, _ = ob.synth_queries(37, base, nq, dim)
+    fs = ob.RankQuantFastscan(dim)
+    fs.add(docs)
+    f, d = _fastscan_modes(
+        monkeypatch, fs, queries, k,
+        filt={"OVB_FASTSCAN_TC": "1", "OVB_FASTSCAN_FILTER": "1"},
+        dense={"OVB_FASTSCAN_TC": "1", "OVB_FASTSCAN_FILTER": "0"},
+    )
+    _same(f, d)
+    s_ref, i_ref = orc.fastscan_search(orc.fastscan_pack(docs, dim), n, dim, queries[:2], k)
+    assert np.array_equal(f.indices.reshape(nq, k)[:2], i_ref)
+    assert np.array_equal(f.scores.reshape(nq, k)[:2].view(np.uint32), s_ref.view(np.uint32))
+
+
 def test_fastscan_reference_formula_corpus(orc):
     """src/fastscan.rs:755-777 corpus (dim 64, n 65, k 9) including a zero query."""
     dim, n, k = 64, 65, 9
@@ -400,6 +474,26 @@ def test_fastscan_full_size_property(orc):
     s_ref, i_ref = orc.fastscan_search(blocks, n, dim, queries, 1000)
     assert np.array_equal(res.indices.reshape(3, 1000), i_ref)
     assert np.array_equal(res.scores.reshape(3, 1000).view(np.uint32), s_ref.view(np.uint32))
+
+
+def test_fastscan_full_size_batched_filter(orc, monkeypatch):
+    """171,332 docs x dim 1024, 300 queries, m = 1000 (the batched two-stage
+    candidate step): the default path (TC scan + threshold filter) equals the
+    key-matrix path bit for bit, and the oracle on a few rows."""
+    n, dim, nq, m = 171_332, 1024, 300, 1000
+    docs = ob.synth_docs(0x0DD5EED2, n, dim)
+    queries, _ = ob.synth_queries(0x0DD5EED2, n, nq, dim)
+    fs = ob.RankQuantFastscan(dim)
+    fs.add(docs)
+    f, d = _fastscan_modes(
+        monkeypatch, fs, queries, m,
+        default={},
+        dense={"OVB_FASTSCAN_FILTER": "0"},
+    )
+    _same(f, d)
+    s_ref, i_ref = orc.fastscan_search(fs.payload(), n, dim, queries[:2], m)
+    assert np.array_equal(f.indices.reshape(nq, m)[:2], i_ref)
+    assert np.array_equal(f.scores.reshape(nq, m)[:2].view(np.uint32), s_ref.view(np.uint32))
 
 
 # ------------------------------------------------------------ Bitmap / sign
