@@ -30,7 +30,9 @@
 //   dense   keys[q][u] = key32 for every logical doc u (the key matrix)
 //   filter  only keys <= thr[q] are appended to row q of a capacity-`cap`
 //           buffer (key, doc id) through an atomic counter; cnt[q] ends as the
-//           number of qualifying docs even when it exceeds `cap`.
+//           number of qualifying docs even when it exceeds `cap`, or with bit
+//           31 set when a tile kept more than its shared-memory list holds
+//           (either way cnt[q] > cap and the caller redoes the query densely).
 // Doc sampling: logical 32-doc block ub reads physical block ub * block_stride,
 // so a stride > 1 scores an evenly spread sample of the index.
 #include <cuda.h>
@@ -57,8 +59,12 @@ constexpr uint32_t kAcc1Col = 256;
 constexpr uint32_t kWaitLimit = 1u << 22;
 constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s
 constexpr uint32_t kSuspendNs = 100000;       // try_wait sleep hint (0.1 ms)
-// filter epilogue list (key, q | slot << 8 | row << 16) in the dead A stages
+constexpr uint32_t kExactCompare = 0xFFFFFFFFu;  // amin: compare keys, not accumulators
+constexpr uint32_t kNeverPasses = 0xFFFFFFFEu;   // amin past the tile's queries (acc < 2^23)
+// filter epilogue list (accumulator, q | slot << 8 | row << 16) in the dead A stages,
+// one segment per epilogue warp
 constexpr uint32_t kListCap = kTcStages * kAStage / 8;
+constexpr uint32_t kSegCap = kListCap / (kTcBuilders / 32);
 
 struct TcSmem {
   uint8_t a[kTcStages][kAStage];
@@ -66,14 +72,16 @@ struct TcSmem {
   float bias[kTcMaxN];
   float invq[kTcMaxN];
   uint32_t thr[kTcMaxN];
+  uint32_t amin[kTcMaxN];  // filter: smallest passing accumulator, or kExactCompare
   uint64_t full_a[kTcStages];
   uint64_t full_b[kTcStages];
   uint64_t empty[kTcStages];
   uint64_t acc_full;
   uint32_t cnt[kTcMaxN];   // filter: kept docs per query in this tile
   uint32_t base[kTcMaxN];  // filter: the tile's first slot in each query row
-  uint32_t list_n;
   uint32_t epi_ok;
+  uint32_t seg_full;   // filter: some warp's list segment overflowed
+  uint32_t any_exact;  // filter: some query of the tile needs key compares
   uint32_t tmem;
   uint32_t abort;
 };
@@ -146,13 +154,20 @@ __device__ __forceinline__ uint64_t global_ns() {
 
 // Bounded parity wait: at most kWaitLimit polls and about kWaitNs of wall
 // time; returns false on timeout.
+// The clock is read only every 256 polls: timer reads are slow and would
+// delay the waiters (the MMA issuer among them) behind each other.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   const uint32_t addr = smem_u32(bar);
-  if (mbar_try(addr, parity)) return true;
-  const uint64_t t0 = global_ns();
+  uint64_t t0 = 0;
   for (uint32_t it = 0; it < kWaitLimit; it++) {
     if (mbar_try(addr, parity)) return true;
-    if (global_ns() - t0 > kWaitNs) return false;
+    if ((it & 255) == 255) {
+      const uint64_t now = global_ns();
+      if (!t0)
+        t0 = now;
+      else if (now - t0 > kWaitNs)
+        return false;
+    }
   }
   return false;
 }
@@ -222,6 +237,43 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Exact f32 value of an accumulator below 2^23 (acc <= 255 * pairs_pad): the
+// integer is placed in the mantissa of 2^23 and 2^23 subtracted; no conversion
+// instruction, same value as a round-to-nearest u32 -> f32 conversion.
+__device__ __forceinline__ float acc_to_float(uint32_t acc) {
+  return __fsub_rn(__uint_as_float(acc | 0x4B000000u), 8388608.0f);
+}
+
+// (bias + acc * inv_q) * inv_norm in f32, round-to-nearest at every step
+// (src/fastscan.rs:306-307: raw = bias_sum + acc * inv_q, then * inv_norm), as
+// the CUDA-core kernel computes it.
+__device__ __forceinline__ float tc_score(uint32_t acc, float bias, float invq, float inv_norm) {
+  return __fmul_rn(__fadd_rn(bias, __fmul_rn(acc_to_float(acc), invq)), inv_norm);
+}
+
+// Filter threshold on the accumulator.  With bias, inv_q, inv_norm finite,
+// inv_q >= 0 and inv_norm > 0, every step of tc_score is monotone
+// non-decreasing in acc (no NaN can arise), so desc_key(score) is non-increasing
+// and {acc : key <= thr} = [amin, amax]; the binary search finds amin
+// (amax + 1 when no accumulator passes).  Otherwise kExactCompare.
+__device__ uint32_t filter_amin(float bias, float invq, float inv_norm, uint32_t thr, uint32_t amax) {
+  if (!(isfinite(bias) && isfinite(invq) && isfinite(inv_norm) && invq >= 0.0f && inv_norm > 0.0f))
+    return kExactCompare;
+  uint32_t lo = 0, hi = amax + 1;
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if (desc_key(tc_score(mid, bias, invq, inv_norm)) <= thr)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(x), "r"(y), "r"(z), "r"(w) : "memory");
+}
+
 __device__ __forceinline__ uint4 load_codes(const uint8_t* p) {
   uint4 v;
   asm volatile("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
@@ -256,8 +308,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     mbar_init(&S.acc_full, 1);
     S.abort = 0;
-    S.list_n = 0;
     S.epi_ok = 1;
+    S.seg_full = 0;
+    S.any_exact = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (uint32_t i = t; i < nt; i += kTcThreads) {
@@ -265,8 +318,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     S.bias[i] = v ? a.bias[q0 + i] : 0.0f;
     S.invq[i] = v ? a.invq[q0 + i] : 0.0f;
     S.thr[i] = (v && !dense) ? a.thr[(q0 + i) * a.thr_stride] : 0u;
+    S.amin[i] = !v ? kNeverPasses
+                   : dense ? kExactCompare : filter_amin(S.bias[i], S.invq[i], a.inv_norm, S.thr[i], 255u * a.pairs_pad);
     S.cnt[i] = 0;
   }
+  __syncthreads();  // barrier init and amin visible to every thread
+  for (uint32_t i = t; i < nt; i += kTcThreads)
+    if (S.amin[i] == kExactCompare) atomicOr(&S.any_exact, 1u);
+  for (uint32_t i = nt + t; i < kTcMaxN; i += kTcThreads) S.amin[i] = kNeverPasses;
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -335,44 +394,50 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const uint64_t pb = ((uint64_t)blockIdx.x * 8 + (r >> 5)) * a.block_stride;
       const bool row_valid = pb < n_blocks;
       const uint8_t* row_codes = a.blocks + pb * (uint64_t)a.pairs_pad * 16 + (uint64_t)(r & 31) * 16;
-      const uint32_t a_off = (r >> 7) * kAHalf + ((r & 127) >> 3) * 1024 + (r & 7) * 128;
-      const uint32_t swz = r & 7;
-      uint4 chunk = make_uint4(0, 0, 0, 0);
-      uint4 next = row_valid ? load_codes(row_codes) : make_uint4(0, 0, 0, 0);
-      for (uint32_t kb = 0; kb < n_kb; kb++) {
-        const uint32_t s = kb % kTcStages, it = kb / kTcStages;
-        if ((kb & 3) == 0) {
-          chunk = next;
-          const uint32_t g = (kb >> 2) + 1;  // next 32-pair group
-          if (row_valid && g * 4 < n_kb) next = load_codes(row_codes + (uint64_t)g * 512);
-        }
-        // warp-uniform control flow: lane 0 waits for the stage, the warp
-        // follows its verdict
-        if (__any_sync(0xFFFFFFFFu, aborted(S))) break;
-        if (kb >= kTcStages) {
-          bool ok = true;
-          if (lane == 0) ok = mbar_wait(&S.empty[s], (it - 1) & 1);
-          ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
-          if (!ok) {
-            if (lane == 0) raise_abort(S, a.err);
-            break;
-          }
-          __syncwarp();
-        }
-        const uint32_t w4 = (kb & 3) == 0 ? chunk.x : (kb & 3) == 1 ? chunk.y : (kb & 3) == 2 ? chunk.z : chunk.w;
-        const uint32_t w = w4 >> (16 * hc);  // this thread's four nibbles
-        uint8_t* arow = S.a[s] + a_off;
+      // shared-space addresses of this thread's four 16-byte chunks in stage 0
+      const uint32_t a_row = smem_u32(S.a[0]) + (r >> 7) * kAHalf + ((r & 127) >> 3) * 1024 + (r & 7) * 128;
+      uint32_t dst[4];
 #pragma unroll
-        for (uint32_t c = 0; c < 4; c++) {
-          const uint32_t sh = c == 0 ? (w << 3) & 0x78u : (w >> (4 * c - 3)) & 0x78u;  // 8 * nibble
-          const uint4 v = make_uint4(shl1(sh), shl1(sh - 32), shl1(sh - 64), shl1(sh - 96));
-          *reinterpret_cast<uint4*>(arow + (((4 * hc + c) ^ swz) << 4)) = v;
+      for (uint32_t c = 0; c < 4; c++) dst[c] = a_row + (((4 * hc + c) ^ (r & 7)) << 4);
+      // one 16-byte code load covers a 32-pair group = 4 K-blocks
+      const uint32_t n_groups = n_kb / 4;
+      uint4 next = row_valid ? load_codes(row_codes) : make_uint4(0, 0, 0, 0);
+      uint32_t s = 0, par = 0, base = 0;  // stage of kb, parity of kb / kTcStages, stage offset
+      bool ok = true;
+      for (uint32_t g = 0; g < n_groups && ok; g++) {
+        const uint4 chunk = next;
+        if (row_valid && g + 1 < n_groups) next = load_codes(row_codes + (uint64_t)(g + 1) * 512);
+#pragma unroll
+        for (uint32_t j = 0; j < 4; j++) {
+          // warp-uniform control flow: lane 0 waits for the stage, the warp
+          // follows its verdict
+          if (4 * g + j >= (uint32_t)kTcStages) {
+            if (lane == 0) ok = mbar_wait(&S.empty[s], par ^ 1);
+            ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
+            if (!ok) {
+              if (lane == 0) raise_abort(S, a.err);
+              break;
+            }
+            __syncwarp();
+          }
+          const uint32_t w = (j == 0 ? chunk.x : j == 1 ? chunk.y : j == 2 ? chunk.z : chunk.w) >> (16 * hc);
+#pragma unroll
+          for (uint32_t c = 0; c < 4; c++) {
+            const uint32_t sh = c == 0 ? (w << 3) & 0x78u : (w >> (4 * c - 3)) & 0x78u;  // 8 * nibble
+            st_shared_v4(dst[c] + base, shl1(sh), shl1(sh - 32), shl1(sh - 64), shl1(sh - 96));
+          }
+          // each lane makes its rows visible to the tensor core's (async) proxy;
+          // the warp barrier orders all lanes before lane 0's release-arrive
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&S.full_a[s]);
+          base += kAStage;
+          if (++s == kTcStages) {
+            s = 0;
+            base = 0;
+            par ^= 1;
+          }
         }
-        // each lane makes its rows visible to the tensor core's (async) proxy;
-        // the warp barrier orders all lanes before lane 0's release-arrive
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&S.full_a[s]);
       }
     }
 
@@ -380,13 +445,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     bool ready = false;
     if (lane == 0) {
       const uint32_t addr = smem_u32(&S.acc_full);
-      const uint64_t t0 = global_ns();
+      uint64_t t0 = 0;
       for (uint32_t it = 0; it < kWaitLimit && !aborted(S); it++) {
         if (mbar_try(addr, 0)) {
           ready = true;
           break;
         }
-        if (global_ns() - t0 > kWaitNs) break;
+        if ((it & 255) == 255) {
+          const uint64_t now = global_ns();
+          if (!t0)
+            t0 = now;
+          else if (now - t0 > kWaitNs)
+            break;
+        }
       }
       if (!ready && !aborted(S)) raise_abort(S, a.err);
     }
@@ -408,52 +479,76 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const uint64_t u = (uint64_t)blockIdx.x * kTcM + row;
       const bool valid = pb < n_blocks && doc < a.n;
       const uint32_t taddr = tmem + ((lq * 32) << 16) + h * kAcc1Col;
-      // filter list: the A stages are dead once acc_full has fired
-      uint2* list = reinterpret_cast<uint2*>(&S.a[0][0]);
+      const bool any_exact = S.any_exact != 0;
+      // filter list: the A stages are dead once acc_full has fired; each warp
+      // appends to its own segment with a register counter (ballot ranks), so
+      // only the per-query slot counters see shared-memory atomics
+      uint2* list = reinterpret_cast<uint2*>(&S.a[0][0]) + (uint32_t)(warp - 2) * kSegCap;
+      uint32_t wcount = 0;
+      uint32_t lt;
+      asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
       for (uint32_t cb = c0; cb < nt; cb += 64) {
         uint32_t v[32];
         __syncwarp();
         tmem_ld32(taddr + cb, v);
-        if (valid) {
+        if (dense) {
 #pragma unroll
           for (uint32_t j = 0; j < 32; j++) {
             const uint32_t q = cb + j;
-            if (q < nqt) {
-              const float sc =
-                  __fmul_rn(__fadd_rn(S.bias[q], __fmul_rn(__uint2float_rn(v[j]), S.invq[q])), a.inv_norm);
-              const uint32_t key = desc_key(sc);
-              if (dense) {
-                a.keys[(q0 + q) * a.ld + u] = key;
-              } else if (key <= S.thr[q]) {
-                const uint32_t e = atom_add_shared(&S.list_n, 1u);
-                if (e < kListCap) {
-                  const uint32_t li = atom_add_shared(&S.cnt[q], 1u);  // < 256: one slot per row
-                  list[e] = make_uint2(key, q | (li << 8) | (row << 16));
-                } else {  // list full: claim a global slot directly
-                  const uint32_t pos = atomicAdd(&a.cnt[q0 + q], 1u);
-                  if (pos < a.cap) {
-                    a.f_keys[(q0 + q) * a.cap + pos] = key;
-                    a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)doc;
-                  }
-                }
-              }
-            }
+            if (valid && q < nqt)
+              a.keys[(q0 + q) * a.ld + u] = desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm));
           }
+          continue;
+        }
+        // filter: 32 independent compares + ballots (amin is kNeverPasses past
+        // nqt), then the appends at prefix offsets of the ballots; no atomics
+        uint32_t m[32];
+        if (!any_exact) {  // the common case: accumulator compares only
+#pragma unroll
+          for (uint32_t j = 0; j < 32; j++) m[j] = __ballot_sync(0xFFFFFFFFu, valid & (v[j] >= S.amin[cb + j]));
+        } else {
+#pragma unroll
+          for (uint32_t j = 0; j < 32; j++) {
+            const uint32_t q = cb + j;  // < kTcMaxN; same q in every lane
+            const uint32_t am = S.amin[q];
+            const bool pass = am != kExactCompare
+                                  ? v[j] >= am
+                                  : desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm)) <= S.thr[q];
+            m[j] = __ballot_sync(0xFFFFFFFFu, valid & pass);
+          }
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < 32; j++) {
+          const uint32_t e = wcount + __popc(m[j] & lt);
+          if (((m[j] >> lane) & 1) && e < kSegCap) list[e] = make_uint2(v[j], (cb + j) | (row << 16));
+          wcount += __popc(m[j]);
         }
       }
       if (!dense) {
-        // one global atomic per query per tile, then the scattered writes
+        // slots within each query's share of the tile (lane-parallel atomics),
+        // one global atomic per query per tile, then each warp writes its segment
+        const uint32_t total = wcount < kSegCap ? wcount : kSegCap;
+        if (wcount > kSegCap && lane == 0) atomicExch(&S.seg_full, 1u);
+        __syncwarp();  // entries were appended by every lane of the warp
+        for (uint32_t e = lane; e < total; e += 32) {
+          const uint32_t y = list[e].y;
+          list[e].y = y | (atom_add_shared(&S.cnt[y & 255], 1u) << 8);  // slot < 256
+        }
         epi_bar();
         const uint32_t i = (uint32_t)t - 64;
-        if (i < nqt && S.cnt[i]) S.base[i] = atomicAdd(&a.cnt[q0 + i], S.cnt[i]);
+        if (i < nqt) {
+          if (S.seg_full)  // some kept doc did not fit: mark every query (bit 31 > cap)
+            atomicOr(&a.cnt[q0 + i], 0x80000000u);  // so the chunk is redone densely
+          else if (S.cnt[i])
+            S.base[i] = atomicAdd(&a.cnt[q0 + i], S.cnt[i]);
+        }
         epi_bar();
-        const uint32_t total = S.list_n < kListCap ? S.list_n : kListCap;
-        for (uint32_t e = i; e < total; e += kTcBuilders) {
-          const uint2 en = list[e];
+        for (uint32_t e = lane; e < total; e += 32) {
+          const uint2 en = list[e];  // (accumulator, q | slot << 8 | row << 16)
           const uint32_t q = en.y & 255, li = (en.y >> 8) & 255, rw = en.y >> 16;
           const uint32_t pos = S.base[q] + li;
           if (pos < a.cap) {
-            a.f_keys[(q0 + q) * a.cap + pos] = en.x;
+            a.f_keys[(q0 + q) * a.cap + pos] = desc_key(tc_score(en.x, S.bias[q], S.invq[q], a.inv_norm));
             const uint64_t rpb = ((uint64_t)blockIdx.x * 8 + (rw >> 5)) * a.block_stride;
             a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw & 31));
           }
@@ -502,6 +597,8 @@ void launch_tc(TcArgs a, const uint8_t* lut, cudaStream_t stream) {
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (rc != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed for the FastScan LUT matrix");
+  if (255ull * a.pairs_pad >= (1ull << 23))  // acc_to_float range
+    throw std::invalid_argument("FastScan tensor-core scan: dimension too large");
   const size_t smem = sizeof(TcSmem) + 1024;
   OVB_CUDA(cudaFuncSetAttribute(fastscan_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const uint64_t n_blocks = (a.n + 31) / 32;
