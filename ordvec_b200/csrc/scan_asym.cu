@@ -27,8 +27,10 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Four independent DFMA chains per lane (code c of a word goes to chain c % 4)
+// so consecutive DFMAs do not wait on each other.
 template <int BITS>
-__device__ __forceinline__ double word_dot(uint32_t x, const double* qs, double acc) {
+__device__ __forceinline__ void word_dot(uint32_t x, const double* qs, double (&acc)[4]) {
   constexpr int CPB = 8 / BITS;
   constexpr uint32_t MASK = (1u << BITS) - 1;
 #pragma unroll
@@ -38,10 +40,9 @@ __device__ __forceinline__ double word_dot(uint32_t x, const double* qs, double 
       const int s = 8 * b + 8 - BITS * (i + 1);
       const uint32_t code = (x >> s) & MASK;
       const double f = __hiloint2double((int)(0x3FF00000u | (code << (20 - BITS))), 0);
-      acc = fma(qs[b * CPB + i], f, acc);
+      acc[(b * CPB + i) & 3] = fma(qs[b * CPB + i], f, acc[(b * CPB + i) & 3]);
     }
   }
-  return acc;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -69,16 +70,31 @@ __device__ __forceinline__ double load_q(const float* qu, uint32_t words, int la
   return warp_sum(s);
 }
 
-template <int BITS, int W>
-__device__ __forceinline__ double row_dot(const uint32_t* row, uint32_t words, int lane,
-                                          const double (&qs)[W][32 / BITS]) {
-  double acc = 0.0;
+// This lane's words of a row (lane + 32 i); zero past the row.
+template <int W>
+__device__ __forceinline__ void load_row(const uint32_t* row, uint32_t words, int lane, uint32_t (&x)[W]) {
 #pragma unroll
   for (int i = 0; i < W; i++) {
     const uint32_t w = lane + i * 32;
-    if (w < words) acc = word_dot<BITS>(__ldcs(row + w), qs[i], acc);
+    x[i] = w < words ? __ldg(row + w) : 0u;
   }
-  return warp_sum(acc);
+}
+
+// Zero words (and the zero query coordinates past the row) add exact zeros.
+template <int BITS, int W>
+__device__ __forceinline__ double words_dot(const uint32_t (&x)[W], const double (&qs)[W][32 / BITS]) {
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int i = 0; i < W; i++) word_dot<BITS>(x[i], qs[i], acc);
+  return warp_sum((acc[0] + acc[1]) + (acc[2] + acc[3]));
+}
+
+template <int BITS, int W>
+__device__ __forceinline__ double row_dot(const uint32_t* row, uint32_t words, int lane,
+                                          const double (&qs)[W][32 / BITS]) {
+  uint32_t x[W];
+  load_row<W>(row, words, lane, x);
+  return words_dot<BITS, W>(x, qs);
 }
 
 template <int BITS>
@@ -120,9 +136,25 @@ __global__ void __launch_bounds__(kThreads)
   const double qsum = load_q<BITS, W>(q_unit + qi * dim, words, lane, qs);
   const uint64_t gw = ((uint64_t)blockIdx.x * kThreads + threadIdx.x) / 32;
   const uint64_t nw = (uint64_t)gridDim.x * kThreads / 32;
-  for (uint64_t i = s + gw; i < e; i += nw) {
-    const double dot = row_dot<BITS, W>((const uint32_t*)codes + (uint64_t)cands[i] * words, words, lane, qs);
+  // software pipeline: the next row's candidate id and words are in flight
+  // while this row is scored
+  const uint32_t* rows = (const uint32_t*)codes;
+  uint64_t i = s + gw;
+  if (i >= e) return;
+  uint32_t x[W];
+  load_row<W>(rows + (uint64_t)cands[i] * words, words, lane, x);
+  uint32_t next_id = i + nw < e ? cands[i + nw] : 0u;
+  for (; i < e; i += nw) {
+    uint32_t y[W];
+    const bool more = i + nw < e;
+    if (more) load_row<W>(rows + (uint64_t)next_id * words, words, lane, y);
+    if (i + 2 * nw < e) next_id = cands[i + 2 * nw];
+    const double dot = words_dot<BITS, W>(x, qs);
     if (lane == 0) keys[i] = finish<BITS>(dot, qsum, inv_norm);
+    if (more) {
+#pragma unroll
+      for (int k = 0; k < W; k++) x[k] = y[k];
+    }
   }
 }
 
