@@ -18,6 +18,8 @@
 // u32 words by a full warp (lane l takes words l, l+32, ...): every warp load
 // is 128 contiguous bytes and each lane's query coordinates never change
 // across rows.
+#include <cstdlib>
+
 #include "ovb_common.cuh"
 #include "ovb_kernels.h"
 
@@ -202,6 +204,130 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// ---- table form ----------------------------------------------------------------
+// Per query, T[n][v] = sum_{i<G} q[nG+i] * (code_i(v) - c) in FP64 for every
+// 4-bit group n of a code row (G = 4 / BITS codes, MSB-first, c = (2^B-1)/2)
+// and every nibble value v; a row's score is inv_norm * sum_n T[n][nib_n(row)].
+// Each entry is a sum of G exact products (q * (code - c) needs at most 27
+// significant bits), so the result agrees with the direct FP64 sum to ~1e-15.
+// Lanes take rows (32 rows per warp) and walk the nibbles in step: a warp's
+// shared-memory read stays inside one 128-byte group of 16 entries (at most 16
+// distinct addresses, one wavefront), and each lane ends with its own row's
+// sum, so no shuffles are needed.  Rows must be whole 16-byte chunks
+// (dim * BITS % 128 == 0); the table (dim * BITS * 32 bytes) sits at a
+// 4096-byte-aligned shared address so a group's address is base | offset.
+constexpr int kTabThreads = 256;
+constexpr uint32_t kTabMaxBytes = 200 * 1024;
+
+__device__ __forceinline__ double lds_f64(uint32_t addr) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr));
+  return v;
+}
+
+template <int BITS, bool SUBSET>
+__global__ void __launch_bounds__(kTabThreads)
+    asym_table_kernel(const uint8_t* __restrict__ codes, uint64_t n, uint32_t dim,
+                      const float* __restrict__ q_unit, const uint64_t* __restrict__ off,
+                      const uint32_t* __restrict__ cands, float inv_norm, uint32_t* __restrict__ keys,
+                      uint64_t ld) {
+  constexpr int G = 4 / BITS;
+  constexpr uint32_t MASK = (1u << BITS) - 1;
+  constexpr double C = ((double)(1u << BITS) - 1.0) * 0.5;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t t_base = ((uint32_t)__cvta_generic_to_shared(smem_raw) + 4095u) & ~4095u;
+  double* T = reinterpret_cast<double*>(smem_raw + (t_base - (uint32_t)__cvta_generic_to_shared(smem_raw)));
+  const uint64_t qi = blockIdx.y;
+  const float* q = q_unit + qi * dim;
+  const uint32_t n_nib = dim * BITS / 4;
+  for (uint32_t e = threadIdx.x; e < n_nib * 16; e += kTabThreads) {
+    const uint32_t g = e >> 4, v = e & 15;
+    double acc = 0.0;
+#pragma unroll
+    for (int i = 0; i < G; i++) {
+      const uint32_t code = (v >> (BITS * (G - 1 - i))) & MASK;
+      acc += (double)q[g * G + i] * ((double)code - C);
+    }
+    T[e] = acc;
+  }
+  __syncthreads();
+
+  uint64_t start, end;
+  if (SUBSET) {
+    start = off[qi];
+    end = off[qi + 1];
+  } else {
+    start = 0;
+    end = n;
+  }
+  const uint32_t bpv = dim * BITS / 8, chunks = bpv / 16;
+  const int lane = threadIdx.x & 31;
+  const uint64_t gw = ((uint64_t)blockIdx.x * kTabThreads + threadIdx.x) / 32;
+  const uint64_t nw = (uint64_t)gridDim.x * kTabThreads / 32;
+  for (uint64_t base = start + gw * 32; base < end; base += nw * 32) {
+    const uint64_t i = base + lane;
+    const bool valid = i < end;
+    const uint64_t row = valid ? (SUBSET ? (uint64_t)cands[i] : i) : 0;
+    const uint4* rp = reinterpret_cast<const uint4*>(codes + row * bpv);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    uint4 x = valid ? __ldg(rp) : make_uint4(0, 0, 0, 0);
+    for (uint32_t c = 0; c < chunks; c++) {
+      const uint4 cur = x;
+      if (c + 1 < chunks) x = valid ? __ldg(rp + c + 1) : make_uint4(0, 0, 0, 0);
+      const uint32_t tb = t_base + c * 4096;  // 32 groups x 128 bytes
+      const uint32_t w[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+#pragma unroll
+          for (int h = 0; h < 2; h++) {  // high nibble first (MSB-first codes)
+            const int sh = 8 * b + (h ? 0 : 4);
+            const uint32_t o = sh >= 3 ? (w[k] >> (sh - 3)) & 0x78u : (w[k] << 3) & 0x78u;  // 8 * nibble
+            const int nl = 8 * k + 2 * b + h;
+            acc[nl & 3] += lds_f64((tb | o) + nl * 128);
+          }
+        }
+      }
+    }
+    if (valid) {
+      const float sc = (float)(((acc[0] + acc[1]) + (acc[2] + acc[3])) * (double)inv_norm);
+      if (SUBSET)
+        keys[i] = desc_key(sc);
+      else
+        keys[qi * ld + i] = desc_key(sc);
+    }
+  }
+}
+
+size_t table_smem(uint32_t dim, uint32_t bits) { return (size_t)dim * bits * 32 + 4096; }
+
+bool table_ok(uint32_t dim, uint32_t bits) {
+  const char* e = getenv("OVB_ASYM_TABLE");
+  if (e && e[0] == '0') return false;
+  return (uint64_t)dim * bits % 128 == 0 && (uint64_t)dim * bits * 32 <= kTabMaxBytes;
+}
+
+template <bool SUBSET>
+void launch_table(uint32_t bits, dim3 grid, size_t smem, cudaStream_t st, const uint8_t* codes, uint64_t n,
+                  uint32_t dim, const float* qu, const uint64_t* off, const uint32_t* cands, float inv_norm,
+                  uint32_t* keys, uint64_t ld) {
+#define OVB_TAB(B)                                                                                     \
+  do {                                                                                                 \
+    OVB_CUDA(cudaFuncSetAttribute(asym_table_kernel<B, SUBSET>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                  (int)smem));                                                         \
+    asym_table_kernel<B, SUBSET><<<grid, kTabThreads, smem, st>>>(codes, n, dim, qu, off, cands, inv_norm, \
+                                                                  keys, ld);                           \
+  } while (0)
+  if (bits == 1)
+    OVB_TAB(1);
+  else if (bits == 2)
+    OVB_TAB(2);
+  else
+    OVB_TAB(4);
+#undef OVB_TAB
+}
+
 unsigned grid_x(uint64_t rows_per_cta, uint64_t n) {
   uint64_t g = (n + rows_per_cta - 1) / rows_per_cta;
   if (g < 1) g = 1;
@@ -261,6 +387,17 @@ void launch_asym_scan(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_t b
                       const float* q_unit, uint64_t nq, float inv_norm, uint32_t* keys,
                       uint64_t ld, cudaStream_t stream) {
   if (!n || !nq) return;
+  if (table_ok(dim, bits)) {
+    // ~1024 rows per CTA: the table build stays a few percent of the scoring
+    for (uint64_t q0 = 0; q0 < nq; q0 += 65535) {
+      unsigned gy = (unsigned)((nq - q0) < 65535 ? (nq - q0) : 65535);
+      dim3 grid(grid_x(1024, n), gy);
+      launch_table<false>(bits, grid, table_smem(dim, bits), stream, codes, n, dim, q_unit + q0 * dim, nullptr,
+                          nullptr, inv_norm, keys + q0 * ld, ld);
+      launched();
+    }
+    return;
+  }
   const int W = plan_w(dim, bits);
   for (uint64_t q0 = 0; q0 < nq; q0 += 65535) {
     unsigned gy = (unsigned)((nq - q0) < 65535 ? (nq - q0) : 65535);
@@ -279,6 +416,20 @@ void launch_asym_subset(const uint8_t* codes, uint32_t dim, uint32_t bits, const
                         uint64_t nq, const uint64_t* offsets, const uint32_t* cands,
                         uint64_t max_row, float inv_norm, uint32_t* keys, cudaStream_t stream) {
   if (!nq || !max_row) return;
+  // the table pays off once several queries share the GPU; a lone query's few
+  // hundred rows are cheaper than its table (the register form below)
+  if (nq >= 16 && table_ok(dim, bits)) {
+    // 512 rows per CTA (two per lane) with many queries, fewer with few
+    const uint64_t rows_per_cta = nq >= 64 ? 512 : 128;
+    for (uint64_t q0 = 0; q0 < nq; q0 += 65535) {
+      unsigned gy = (unsigned)((nq - q0) < 65535 ? (nq - q0) : 65535);
+      dim3 grid(grid_x(rows_per_cta, max_row), gy);
+      launch_table<true>(bits, grid, table_smem(dim, bits), stream, codes, 0, dim, q_unit + q0 * dim,
+                         offsets + q0, cands, inv_norm, keys, 0);
+      launched();
+    }
+    return;
+  }
   const int W = plan_w(dim, bits);
   // each warp loads its query slice once, so give it ~32 rows when there are
   // many queries; a single query spreads its rows over more CTAs
