@@ -115,8 +115,8 @@ def cpu_two_stage_qps(docs, queries, budget_s: float):
 
 
 def reference_arm(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    # the reference path is a CPU path: under torchrun rank 0 alone runs it
+    if int(os.environ.get("RANK", "0")) != 0:
         return
     import ordvec_b200 as ob
     from oracle import oracle as orc
@@ -170,27 +170,21 @@ def main():
     import ordvec_b200 as ob
     from ordvec_b200._lib import check, lib
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from ordvec_b200.replicas import ReplicaGroup, rank_env, shard_seed, whole_job_rate
+
+    rank, world, local = rank_env()
     torch.cuda.set_device(local)
     ob.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    group = ReplicaGroup("nccl", device=dev, sync=lambda: torch.cuda.synchronize(dev))
 
     docs = ob.synth_docs(SEED, N_DOCS, DIM)
-    queries, planted = ob.synth_queries(SEED + 1000 * rank, N_DOCS, NQ, DIM)
+    queries, planted = ob.synth_queries(shard_seed(SEED, rank), N_DOCS, NQ, DIM)
     rq = ob.RankQuant(DIM, 2)
     rq.add(docs)
     fs = ob.RankQuantFastscan(DIM)
     fs.add(docs)
 
-    dev = torch.device("cuda", local)
     d_q = torch.from_numpy(queries).to(dev)
     d_s = torch.empty(NQ * K, dtype=torch.float32, device=dev)
     d_i = torch.empty(NQ * K, dtype=torch.int64, device=dev)
@@ -202,17 +196,8 @@ def main():
         ob.two_stage_search_device(rq, fs, q_ptr or d_q.data_ptr(), nq, M, K, s_ptr or d_s.data_ptr(),
                                    i_ptr or d_i.data_ptr(), sp)
 
-    def barrier():
-        torch.cuda.synchronize(dev)
-        if dist:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = group.barrier
+    max_over_ranks = group.max_over_ranks
 
     for _ in range(args.warmup):
         step_device()
@@ -308,8 +293,8 @@ def main():
                 "queries_per_launch": nq, "algorithmic_ops_per_launch": ops, "launch_ms": ms,
                 "peak_source": f"2 x {peak_kind} bf16 dense TFLOP/s (burst)"}
 
-    value = world * NQ * args.steps / (total_ms * 1e-3)
-    e2e = world * NQ * args.steps / (e2e_total * 1e-3)
+    value = whole_job_rate(NQ * args.steps, world, total_ms)
+    e2e = whole_job_rate(NQ * args.steps, world, e2e_total)
     plain_qps = 1e3 / statistics.mean(plain_ms)
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
@@ -337,9 +322,7 @@ def main():
         qps, threads, sample, _, _, _ = cpu_two_stage_qps(docs, queries, args.cpu_seconds)
         line["cpu_baseline"] = {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
                                 "sample": f"first {sample} of the step's {NQ} queries, all host threads"}
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    group.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
