@@ -261,6 +261,57 @@ ordvec_status_t ovb_synth_queries(uint64_t seed, uint64_t n_docs, uint64_t nq, u
                                   float doc_sigma, float query_sigma, float *out,
                                   uint64_t *planted);
 
+/* ---- Serving loop (no counterpart in the reference) ----------------------
+ * A request server over device-resident indices.  Requests (a block of
+ * queries, k, and m = stage-1 candidates) are queued by ovb_server_submit and
+ * answered by worker threads, each with its own CUDA stream: a free worker
+ * takes the oldest pending request and batches every other pending request of
+ * the same route, k and m behind it (up to max_batch queries: continuous
+ * batching), admits the batch when the device bytes of all batches in flight
+ * stay within hbm_budget_bytes, and runs it while other workers' batches run
+ * on their streams.  A request's results are the ones it gets alone: every
+ * kernel scores a query independently of the others in its batch. */
+typedef struct ovb_server ovb_server_t;
+
+typedef struct ovb_server_config_t {
+    uint64_t struct_size;      /* sizeof(ovb_server_config_t) */
+    uint32_t workers;          /* concurrent batches (streams); 0 -> 2 */
+    uint32_t max_batch;        /* queries per batch; 0 -> 1024 */
+    uint64_t hbm_budget_bytes; /* device bytes of the batches in flight; 0 -> 4 GiB */
+    uint64_t reserved[5];      /* must be zero */
+} ovb_server_config_t;
+
+typedef struct ovb_server_stats_t {
+    uint64_t struct_size;       /* sizeof(ovb_server_stats_t) */
+    uint64_t requests;          /* completed requests */
+    uint64_t queries;           /* completed queries */
+    uint64_t batches;           /* batches run */
+    uint64_t peak_inflight_bytes;
+    uint64_t max_concurrent_batches;
+    double p50_ms, p99_ms, mean_ms; /* submit -> results ready, per request */
+    uint64_t reserved[4];
+} ovb_server_stats_t;
+
+ordvec_status_t ovb_server_new(const ovb_server_config_t *config, ovb_server_t **out);
+/* A route is a RankQuant index searched in full (stage1 NULL) or a
+ * two-stage pair (stage-1 SignBitmap / Bitmap / FastScan / MultiBucket index
+ * -> RankQuant rerank).  Indices must outlive the server. */
+ordvec_status_t ovb_server_add_route(ovb_server_t *server, const ordvec_index_t *rq,
+                                     const ordvec_index_t *stage1, uint32_t *route_out);
+/* Copies nq x dim queries; m = 0 applies the default candidate policy.  Fails
+ * fast on bad arguments or non-finite queries (NONFINITE_QUERY). */
+ordvec_status_t ovb_server_submit(ovb_server_t *server, uint32_t route, const float *queries,
+                                  uint64_t nq, uint64_t k, uint64_t m, uint64_t *ticket_out);
+/* Blocks until the request is answered; writes nq x k_out scores and ids
+ * (k_out = min(k, candidates); capacity = entries available in each array).
+ * A ticket can be waited on once. */
+ordvec_status_t ovb_server_wait(ovb_server_t *server, uint64_t ticket, float *scores,
+                                int64_t *ids, uint64_t capacity, uint64_t *k_out,
+                                double *latency_ms);
+ordvec_status_t ovb_server_stats(ovb_server_t *server, ovb_server_stats_t *out);
+/* Drains the queue (pending requests still run), joins the workers. */
+void ovb_server_free(ovb_server_t *server);
+
 #ifdef __cplusplus
 }
 #endif

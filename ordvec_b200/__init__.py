@@ -5,12 +5,12 @@ Device-resident indices and CUDA kernels behind the reference's C ABI
 """
 from ._lib import LIB_PATH, OrdvecError, lib
 from .api import (Bitmap, CandidateBatch, MultiBucketBitmap, RankQuant, RankQuantFastscan,
-                  SearchResults, SignBitmap, TwoStageCandidatePolicy, last_launch_count, load,
+                  SearchResults, Server, SignBitmap, Ticket, TwoStageCandidatePolicy, last_launch_count, load,
                   set_device, synth_docs, synth_queries, two_stage_profile, two_stage_search,
                   two_stage_search_device)
 
 __all__ = [
     "Bitmap", "CandidateBatch", "MultiBucketBitmap", "OrdvecError", "RankQuant", "RankQuantFastscan",
     "SearchResults", "SignBitmap", "TwoStageCandidatePolicy", "LIB_PATH", "last_launch_count", "lib",
-    "load", "synth_docs", "synth_queries", "two_stage_search",
+    "load", "synth_docs", "synth_queries", "two_stage_search", "Server", "Ticket",
 ]

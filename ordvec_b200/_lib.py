@@ -56,6 +56,18 @@ class SearchStats(C.Structure):
                 ("reserved", C.c_uint64 * 8)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("struct_size", C.c_uint64), ("workers", C.c_uint32), ("max_batch", C.c_uint32),
+                ("hbm_budget_bytes", C.c_uint64), ("reserved", C.c_uint64 * 5)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("struct_size", C.c_uint64), ("requests", C.c_uint64), ("queries", C.c_uint64),
+                ("batches", C.c_uint64), ("peak_inflight_bytes", C.c_uint64),
+                ("max_concurrent_batches", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("mean_ms", C.c_double), ("reserved", C.c_uint64 * 4)]
+
+
 class Hit(C.Structure):
     _fields_ = [("row_id", C.c_uint64), ("id", C.c_uint64), ("score", C.c_float), ("reserved", C.c_uint32)]
 
@@ -104,6 +116,12 @@ SIGNATURES = {
     "ovb_set_device": (S, [C.c_int]),
     "ovb_synth_docs": (S, [U64, U64, U64, U32, F, P]),
     "ovb_synth_queries": (S, [U64, U64, U64, U32, F, F, P, P]),
+    "ovb_server_new": (S, [P, P]),
+    "ovb_server_add_route": (S, [P, P, P, P]),
+    "ovb_server_submit": (S, [P, U32, P, U64, U64, U64, P]),
+    "ovb_server_wait": (S, [P, U64, P, P, U64, P, P]),
+    "ovb_server_stats": (S, [P, P]),
+    "ovb_server_free": (None, [P]),
 }
 
 _lib = None

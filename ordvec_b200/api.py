@@ -17,6 +17,7 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
+from . import _lib as _lib_mod
 from ._lib import (KIND_BITMAP, KIND_FASTSCAN, KIND_MULTIBUCKET, KIND_RANK_QUANT, KIND_SIGN_BITMAP,
                    IndexInfo, OrdvecError, check, lib)
 
@@ -398,6 +399,75 @@ def two_stage_search(rq: RankQuant, stage1: _Index, queries, m: int, k: int) -> 
     i = np.empty(max(nq * ke, 1), np.int64)
     check(lib().ovb_two_stage_search(rq.handle, stage1.handle, _ptr(q), nq, m, k, _ptr(s), _ptr(i)))
     return SearchResults(s[: nq * ke], i[: nq * ke], nq, ke)
+
+
+class Server:
+    """Serving loop over device-resident indices (ovb_server_*): requests are
+    queued, batched with other pending requests of the same route, k and m
+    (continuous batching), admitted under an HBM budget and run by worker
+    threads on their own CUDA streams.  A request's result is the one it gets
+    alone."""
+
+    def __init__(self, workers: int = 2, max_batch: int = 1024, hbm_budget_bytes: int = 0):
+        cfg = _lib_mod.ServerConfig()
+        cfg.struct_size = C.sizeof(_lib_mod.ServerConfig)
+        cfg.workers, cfg.max_batch, cfg.hbm_budget_bytes = workers, max_batch, hbm_budget_bytes
+        h = C.c_void_p()
+        check(lib().ovb_server_new(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._dims: List[int] = []
+        self._keep = []  # indices must outlive the server
+
+    def add_route(self, rq: "RankQuant", stage1: Optional["_Index"] = None) -> int:
+        r = C.c_uint32()
+        check(lib().ovb_server_add_route(self._h, rq.handle, stage1.handle if stage1 is not None else None,
+                                         C.byref(r)))
+        self._dims.append(rq.dim)
+        self._keep.append((rq, stage1))
+        return r.value
+
+    def submit(self, route: int, queries, k: int, m: int = 0) -> "Ticket":
+        if not 0 <= route < len(self._dims):
+            raise OrdvecError(2, "unknown route")  # the status ovb_server_submit returns
+        q = _rows(queries, self._dims[route])
+        nq = q.size // self._dims[route]
+        t = C.c_uint64()
+        check(lib().ovb_server_submit(self._h, route, _ptr(q), nq, k, m, C.byref(t)))
+        return Ticket(self, t.value, nq, k)
+
+    def stats(self) -> dict:
+        st = _lib_mod.ServerStats()
+        st.struct_size = C.sizeof(_lib_mod.ServerStats)
+        check(lib().ovb_server_stats(self._h, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in _lib_mod.ServerStats._fields_ if f not in ("struct_size", "reserved")}
+
+    def close(self) -> None:
+        if self._h:
+            lib().ovb_server_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Ticket:
+    """A submitted request; wait() blocks until its results are ready."""
+
+    def __init__(self, server: Server, ticket: int, nq: int, k: int):
+        self.server, self.ticket, self.nq, self.k = server, ticket, nq, k
+
+    def wait(self):
+        cap = max(self.nq * self.k, 1)
+        s = np.empty(cap, np.float32)
+        i = np.empty(cap, np.int64)
+        ko = C.c_uint64()
+        lat = C.c_double()
+        check(lib().ovb_server_wait(self.server._h, self.ticket, _ptr(s), _ptr(i), cap, C.byref(ko), C.byref(lat)))
+        n = self.nq * ko.value
+        return SearchResults(s[:n], i[:n], self.nq, ko.value), lat.value
 
 
 def synth_docs(seed: int, n: int, dim: int, sigma: float = 0.3, first: int = 0) -> np.ndarray:

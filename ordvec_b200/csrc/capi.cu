@@ -198,6 +198,7 @@ uint32_t bitmap_subset(const Index& bm, const float* d_q, uint64_t nq, const uin
 }  // namespace
 
 ordvec_status_t api_boundary(const std::function<void()>& f) { return boundary(f); }
+void check_tc_errors(Workspace& w) { check_tc(w); }
 
 Workspace::Workspace() {
   OVB_CUDA(cudaGetDevice(&device));

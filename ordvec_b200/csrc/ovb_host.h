@@ -3,6 +3,7 @@
 #pragma once
 #include <stdint.h>
 
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -153,5 +154,10 @@ void read_payload(const Index& ix, std::vector<uint8_t>& out);
 void upload_payload(Index& ix, const uint8_t* payload, uint64_t bytes);
 
 extern thread_local uint64_t tl_last_launches;
+
+// C-ABI error boundary (status + thread-local message) for entry points in
+// other files; tensor-core error word check after a synchronised pipeline.
+ordvec_status_t api_boundary(const std::function<void()>& f);
+void check_tc_errors(Workspace& w);
 
 }  // namespace ovb

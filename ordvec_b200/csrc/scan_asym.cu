@@ -416,9 +416,9 @@ void launch_asym_subset(const uint8_t* codes, uint32_t dim, uint32_t bits, const
                         uint64_t nq, const uint64_t* offsets, const uint32_t* cands,
                         uint64_t max_row, float inv_norm, uint32_t* keys, cudaStream_t stream) {
   if (!nq || !max_row) return;
-  // the table pays off once several queries share the GPU; a lone query's few
-  // hundred rows are cheaper than its table (the register form below)
-  if (nq >= 16 && table_ok(dim, bits)) {
+  // one arithmetic for every batch size, so a query scores the same alone and
+  // inside a batch
+  if (table_ok(dim, bits)) {
     // 512 rows per CTA (two per lane) with many queries, fewer with few
     const uint64_t rows_per_cta = nq >= 64 ? 512 : 128;
     for (uint64_t q0 = 0; q0 < nq; q0 += 65535) {

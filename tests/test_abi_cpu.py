@@ -152,3 +152,23 @@ def test_device_entry_points_fail_cleanly_without_a_gpu():
     assert "CUDA" in L.ordvec_last_error().decode()
     with pytest.raises(ob.OrdvecError):
         ob.RankQuant(64, 2)
+
+
+def test_server_config_is_validated_before_device_use():
+    from ordvec_b200._lib import ServerConfig, ServerStats
+
+    L = lib()
+    assert C.sizeof(ServerConfig) == 64 and C.sizeof(ServerStats) == 104
+    h = C.c_void_p()
+    assert L.ovb_server_new(None, C.byref(h)) == 1
+    cfg = ServerConfig()
+    cfg.struct_size = 8
+    assert L.ovb_server_new(C.byref(cfg), C.byref(h)) == 3
+    cfg.struct_size = C.sizeof(ServerConfig)
+    cfg.reserved[2] = 1
+    assert L.ovb_server_new(C.byref(cfg), C.byref(h)) == 2
+    cfg.reserved[2] = 0
+    cfg.workers = 65
+    assert L.ovb_server_new(C.byref(cfg), C.byref(h)) == 2
+    assert L.ovb_server_submit(None, 0, None, 0, 1, 0, C.byref(C.c_uint64())) == 1
+    L.ovb_server_free(None)  # NULL is a no-op

@@ -570,6 +570,30 @@ def test_two_stage_sign_b1_and_fastscan_b2(orc):
         check_float_topk(res.indices_for_query(qi), res.scores_for_query(qi), cands[qi], s64, k)
 
 
+def test_sign_b1_two_stage_full_size(orc):
+    """The sign-bitmap -> b=1 rerank configuration at full size (N=100,000, dim 1024,
+    k=10, default 320 candidates): one query per call equals the batched call, and
+    both match the oracle (candidates bit-exact, rerank within the FP64 bar)."""
+    n, dim, nq, k = 100_000, 1024, 64, 10
+    docs = ob.synth_docs(0x0DD5EED1, n, dim)
+    queries, _ = ob.synth_queries(0x0DD5EED1, n, nq, dim)
+    sb, rq1 = ob.SignBitmap(dim), ob.RankQuant(dim, 1)
+    sb.add(docs)
+    rq1.add(docs)
+    batched = ob.two_stage_search(rq1, sb, queries, 0, k)
+    words = orc.sign_encode(docs, dim)
+    p1 = orc.rankquant_encode(docs, dim, 1)
+    for qi in range(nq):
+        s, i = rq1.try_search_with_sign_probe(sb, queries[qi], k)
+        assert np.array_equal(i, batched.indices_for_query(qi))
+        assert np.array_equal(s.view(np.uint32), batched.scores_for_query(qi).view(np.uint32))
+    for qi in (0, 17, 63):
+        cand = orc.sign_top_m(words, n, dim, queries[qi], 320)
+        assert np.array_equal(sb.top_m_candidates(queries[qi], 320), cand)
+        s64 = orc.rq_scores_f64_subset(p1, dim, 1, queries[qi], cand)
+        check_float_topk(batched.indices_for_query(qi), batched.scores_for_query(qi), cand, s64, k)
+
+
 def test_two_stage_bitmap_and_multibucket(orc):
     n, dim, nq, k, m = 8000, 768, 4, 20, 500
     docs = ob.synth_docs(0x0DD5EED4, n, dim)
