@@ -154,6 +154,61 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ serving
+def serving_run(ob, rq, fs, queries, batched_ids, seconds: float, rate_qps: float):
+    """The serving loop on this workload's route: seeded Poisson request
+    arrivals offering `rate_qps` queries/s, 1-256 queries per request, k=10,
+    m=1000; answered by ob.Server (continuous batching, 3 worker streams).
+    Reports completed QPS, request latency p50/p99 and whether every answer
+    equals the batched form's top-10."""
+    import threading
+
+    rng = np.random.default_rng(SEED)
+    mean_size = 128.5
+    n_req = max(int(seconds * rate_qps / mean_size), 8)
+    sizes = rng.integers(1, 257, n_req)
+    offs = rng.integers(0, NQ - 256, n_req)
+    gaps = rng.exponential(mean_size / rate_qps, n_req)
+    srv = ob.Server(workers=3, max_batch=1024)
+    route = srv.add_route(rq, fs)
+    srv.wait_ready()  # workers have sized their buffers for the route
+    tickets, done_at, lat = [None] * n_req, [0.0] * n_req, [0.0] * n_req
+    same = [True]
+
+    def collect():
+        for j in range(n_req):
+            while tickets[j] is None:
+                time.sleep(20e-6)
+            res, lat[j] = tickets[j].wait()
+            done_at[j] = time.perf_counter()
+            o, sz = int(offs[j]), int(sizes[j])
+            if not np.array_equal(res.indices.reshape(sz, K), batched_ids[o:o + sz]):
+                same[0] = False
+
+    th = threading.Thread(target=collect)
+    th.start()
+    t0 = time.perf_counter()
+    due = t0
+    for j in range(n_req):
+        due += gaps[j]
+        while time.perf_counter() < due:
+            pass
+        o, sz = int(offs[j]), int(sizes[j])
+        tickets[j] = srv.submit(route, queries[o:o + sz], K, M)
+    th.join()
+    wall = max(done_at) - t0
+    st = srv.stats()
+    srv.close()
+    n_q = int(sizes.sum())
+    return {"offered_qps": rate_qps, "completed_qps": n_q / wall, "requests": n_req, "queries": n_q,
+            "request_queries": "uniform 1-256", "k": K, "candidates": M,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(np.mean(lat)), "batches": st["batches"],
+            "max_concurrent_batches": st["max_concurrent_batches"], "workers": 3,
+            "arrivals": "seeded Poisson", "latency": "submit -> results ready, per request",
+            "identical_top10_vs_batched": same[0]}
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -164,6 +219,8 @@ def main():
     ap.add_argument("--plain-queries", type=int, default=200)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--serve-rate", type=float, default=150_000.0, help="offered queries/s")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -257,6 +314,8 @@ def main():
     plain_ms = [a.elapsed_time(b) for a, b in pev]
     plain_launches = ob.last_launch_count()
     identical = bool(np.array_equal(p_i.view(P, K).cpu().numpy(), batched_ids[:P]))
+    serving = serving_run(ob, rq, fs, queries, batched_ids, args.serve_seconds, args.serve_rate) \
+        if args.serve_seconds > 0 else None
     clock_info = clocks.stop()
 
     # ---- stage profile (roofline of the dominant kernel)
@@ -317,6 +376,7 @@ def main():
         "plain": {"qps": plain_qps, "p50_ms": float(np.percentile(plain_ms, 50)),
                   "p99_ms": float(np.percentile(plain_ms, 99)), "queries": P, "launches_per_query": plain_launches,
                   "identical_top10_vs_batched": identical, "batched_over_plain": value / world / plain_qps},
+        "serving": serving,
         "stages_ms": dict(zip(STAGES, stages)),
         "stages_ms_plain": dict(zip(STAGES, stages1)),
         "scan_gbs_effective": NQ * ref_code_bytes / (stages[2] * 1e-3) / 1e9,

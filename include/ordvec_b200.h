@@ -270,7 +270,10 @@ ordvec_status_t ovb_synth_queries(uint64_t seed, uint64_t n_docs, uint64_t nq, u
  * batching), admits the batch when the device bytes of all batches in flight
  * stay within hbm_budget_bytes, and runs it while other workers' batches run
  * on their streams.  A request's results are the ones it gets alone: every
- * kernel scores a query independently of the others in its batch. */
+ * kernel scores a query independently of the others in its batch.  Before a
+ * worker serves a route it sizes its buffers with two synthetic batches
+ * (31 and max_batch queries, k = 100), so buffer growth (whose frees wait for
+ * the whole device) does not stall batches in flight. */
 typedef struct ovb_server ovb_server_t;
 
 typedef struct ovb_server_config_t {
@@ -289,7 +292,8 @@ typedef struct ovb_server_stats_t {
     uint64_t peak_inflight_bytes;
     uint64_t max_concurrent_batches;
     double p50_ms, p99_ms, mean_ms; /* submit -> results ready, per request */
-    uint64_t reserved[4];
+    uint64_t warm_workers;      /* workers whose buffers are sized for every route */
+    uint64_t reserved[3];
 } ovb_server_stats_t;
 
 ordvec_status_t ovb_server_new(const ovb_server_config_t *config, ovb_server_t **out);

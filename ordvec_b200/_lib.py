@@ -65,7 +65,7 @@ class ServerStats(C.Structure):
     _fields_ = [("struct_size", C.c_uint64), ("requests", C.c_uint64), ("queries", C.c_uint64),
                 ("batches", C.c_uint64), ("peak_inflight_bytes", C.c_uint64),
                 ("max_concurrent_batches", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
-                ("mean_ms", C.c_double), ("reserved", C.c_uint64 * 4)]
+                ("mean_ms", C.c_double), ("warm_workers", C.c_uint64), ("reserved", C.c_uint64 * 3)]
 
 
 class Hit(C.Structure):

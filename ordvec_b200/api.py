@@ -415,6 +415,7 @@ class Server:
         h = C.c_void_p()
         check(lib().ovb_server_new(C.byref(cfg), C.byref(h)))
         self._h = h
+        self.workers = workers if workers else 2
         self._dims: List[int] = []
         self._keep = []  # indices must outlive the server
 
@@ -434,6 +435,16 @@ class Server:
         t = C.c_uint64()
         check(lib().ovb_server_submit(self._h, route, _ptr(q), nq, k, m, C.byref(t)))
         return Ticket(self, t.value, nq, k)
+
+    def wait_ready(self, timeout_s: float = 60.0) -> None:
+        """Block until every worker has sized its buffers for every route."""
+        import time
+
+        t_end = time.monotonic() + timeout_s
+        while self.stats()["warm_workers"] < self.workers:
+            if time.monotonic() > t_end:
+                raise TimeoutError("server workers did not finish sizing their buffers")
+            time.sleep(0.002)
 
     def stats(self) -> dict:
         st = _lib_mod.ServerStats()

@@ -66,7 +66,7 @@ struct Server : ovb_server {
   bool stopping = false;
   uint64_t inflight = 0, peak_inflight = 0;
   uint32_t running = 0, max_running = 0;
-  uint64_t n_req = 0, n_q = 0, n_batches = 0;
+  uint64_t n_req = 0, n_q = 0, n_batches = 0, warm_workers = 0;
   std::vector<double> latencies;
   std::vector<std::thread> threads;
 };
@@ -125,17 +125,52 @@ void run_batch(Server& S, const Route& rt, std::vector<ReqPtr>& batch, uint64_t 
   }
 }
 
+// Grow this worker's device and pinned buffers to a route's largest batch
+// before it serves requests: buffers only grow, and a growth frees the old
+// allocation, which waits for the whole device and would stall the other
+// workers' batches mid-stream.  Both stage-1 forms are exercised (the <32-query
+// CUDA-core scan with its key rows, and a max_batch tensor-core batch).
+void warm_route(Server& S, const Route& rt, HostBuf& hq, HostBuf& hs, HostBuf& hi, DevBuf& dq, DevBuf& ds,
+                DevBuf& di) {
+  const uint32_t dim = rt.rq->dim;
+  for (uint64_t nq : {(uint64_t)31, (uint64_t)S.max_batch}) {
+    std::vector<ReqPtr> batch(1, std::make_shared<Request>());
+    Request& q = *batch[0];
+    q.nq = nq;
+    q.k = 100;
+    q.m = 0;
+    q.q.resize(nq * dim);
+    uint64_t x = 0x9E3779B97F4A7C15ull;
+    for (float& v : q.q) {  // deterministic, finite, non-degenerate
+      x ^= x << 13;
+      x ^= x >> 7;
+      x ^= x << 17;
+      v = (float)((int64_t)(x >> 40) - (1 << 23)) * (1.0f / (1 << 23));
+    }
+    run_batch(S, rt, batch, nq, hq, hs, hi, dq, ds, di);
+  }
+}
+
 void worker_main(Server* S) {
   cudaSetDevice(S->device);
   HostBuf hq, hs, hi;
   DevBuf dq, ds, di;
+  size_t warmed = 0;  // routes this worker has pre-sized its buffers for
   for (;;) {
     std::vector<ReqPtr> batch;
     uint64_t nq = 0, bytes = 0;
     Route rt{};
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      S->cv_work.wait(lk, [&] { return S->stopping || !S->pending.empty(); });
+      S->cv_work.wait(lk, [&] { return S->stopping || !S->pending.empty() || warmed < S->routes.size(); });
+      if (warmed < S->routes.size()) {
+        const Route w = S->routes[warmed++];
+        lk.unlock();
+        api_boundary([&] { warm_route(*S, w, hq, hs, hi, dq, ds, di); });
+        lk.lock();
+        if (warmed == S->routes.size()) S->warm_workers++;
+        continue;
+      }
       if (S->pending.empty()) return;  // stopping and drained
       // the oldest request, then every later one with the same route, k, m
       const ReqPtr head = S->pending.front();
@@ -238,6 +273,8 @@ ordvec_status_t ovb_server_add_route(ovb_server_t* server, const ordvec_index_t*
     std::lock_guard<std::mutex> lk(S.mu);
     S.routes.push_back(Route{&r, s1});
     *route_out = (uint32_t)(S.routes.size() - 1);
+    S.warm_workers = 0;      // every worker now has a route to pre-size for
+    S.cv_work.notify_all();
   });
 }
 
@@ -312,6 +349,7 @@ ordvec_status_t ovb_server_stats(ovb_server_t* server, ovb_server_stats_t* out) 
     out->batches = S.n_batches;
     out->peak_inflight_bytes = S.peak_inflight;
     out->max_concurrent_batches = S.max_running;
+    out->warm_workers = S.warm_workers;
     out->p50_ms = percentile(S.latencies, 0.50);
     out->p99_ms = percentile(S.latencies, 0.99);
     double sum = 0.0;

@@ -63,6 +63,8 @@ def test_server_answers_equal_alone_answers():
     srv = ob.Server(workers=3, max_batch=256)
     ids = [srv.add_route(rq, s1) for rq, s1 in routes]
     assert ids == list(range(len(routes)))
+    srv.wait_ready()
+    assert srv.stats()["warm_workers"] == 3
     rng = np.random.default_rng(11)
     tickets = [None] * len(reqs)
 
