@@ -176,6 +176,16 @@ ordvec_status_t ovb_index_payload(const ordvec_index_t *index, void *out, uint64
 /* RankQuant::search_asymmetric (src/quant.rs:713-847). */
 ordvec_status_t ovb_rankquant_search(const ordvec_index_t *rq, const float *queries,
                                      uint64_t nq, uint64_t k, float *scores, int64_t *ids);
+/* The same full search scored by the split-BF16 tensor-core scan (no
+ * counterpart in the reference): rank codes exact in BF16, the query split
+ * into hi + lo BF16 parts, f32 accumulation; dim must be a multiple of 64.
+ * exact = 1 rescores in FP64 every candidate within twice the split error
+ * bound of the k-th split score, giving ovb_rankquant_search's results
+ * (ovb_rankquant_search itself takes this path for >= 64 queries);
+ * exact = 0 returns the split-BF16 scores and their top-k. */
+ordvec_status_t ovb_rankquant_search_split(const ordvec_index_t *rq, const float *queries,
+                                           uint64_t nq, uint64_t k, uint32_t exact,
+                                           float *scores, int64_t *ids);
 /* RankQuant::search_asymmetric_subset_batched_serial_into (src/quant.rs:1336-1394):
  * CSR candidates (offsets[nq+1]), output nq x min(k, n). */
 ordvec_status_t ovb_rankquant_search_subset(const ordvec_index_t *rq, const float *queries,

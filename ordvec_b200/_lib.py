@@ -116,6 +116,7 @@ SIGNATURES = {
     "ovb_set_device": (S, [C.c_int]),
     "ovb_synth_docs": (S, [U64, U64, U64, U32, F, P]),
     "ovb_synth_queries": (S, [U64, U64, U64, U32, F, F, P, P]),
+    "ovb_rankquant_search_split": (S, [P, P, U64, U64, U32, P, P]),
     "ovb_server_new": (S, [P, P]),
     "ovb_server_add_route": (S, [P, P, P, P]),
     "ovb_server_submit": (S, [P, U32, P, U64, U64, U64, P]),

@@ -198,6 +198,20 @@ class RankQuant(_Index):
             return SearchResults(np.zeros(0, np.float32), np.full(0, -1, np.int64), nq, 0)
         return SearchResults(s[: nq * ke], i[: nq * ke], nq, ke)
 
+    def search_asymmetric_split(self, queries, k: int, exact: bool = True) -> SearchResults:
+        """Full search scored on the tensor cores in split-BF16 (query = hi + lo
+        BF16, codes exact in BF16, f32 accumulation).  exact=True rescores
+        the candidates within the split error bound in FP64 (same results as
+        search_asymmetric); exact=False returns the split-BF16 scores."""
+        dim = self.dim
+        q = _rows(queries, dim)
+        nq = q.size // dim
+        ke = min(k, len(self))
+        s = np.empty(max(nq * ke, 1), np.float32)
+        i = np.empty(max(nq * ke, 1), np.int64)
+        check(lib().ovb_rankquant_search_split(self._h, _ptr(q), nq, ke, 1 if exact else 0, _ptr(s), _ptr(i)))
+        return SearchResults(s[: nq * ke], i[: nq * ke], nq, ke)
+
     def search_asymmetric_subset_batched_serial(self, queries, candidate_offsets, candidates, k) -> SearchResults:
         """src/quant.rs:1336-1451: rectangular nq x min(k, n), sentinel padded."""
         dim = self.dim

@@ -605,6 +605,21 @@ ordvec_status_t ovb_rankquant_search(const ordvec_index_t* rq, const float* quer
   });
 }
 
+ordvec_status_t ovb_rankquant_search_split(const ordvec_index_t* rq, const float* queries, uint64_t nq, uint64_t k,
+                                           uint32_t exact, float* scores, int64_t* ids) {
+  return boundary([&] {
+    const Index& ix = as_index(rq);
+    need_queries(queries, nq);
+    const uint64_t ke = k < ix.n ? k : ix.n;
+    if (!ke || !nq) return;
+    if (!scores || !ids) fail(ORDVEC_STATUS_NULL_POINTER, "output pointer is NULL");
+    Workspace& w = workspace();
+    const float* d_q = upload_queries(w, queries, nq, ix.dim, true);
+    uint32_t got = engine_rankquant_full_split(ix, d_q, nq, ke, exact != 0, w, w.stream);
+    download_results(w, nq * got, 0, 0, scores, ids);
+  });
+}
+
 ordvec_status_t ovb_rankquant_search_subset(const ordvec_index_t* rq, const float* queries, uint64_t nq,
                                             const uint64_t* offsets, const uint32_t* candidates, uint64_t k,
                                             float* scores, int64_t* ids) {

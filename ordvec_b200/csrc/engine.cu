@@ -5,6 +5,7 @@
 // thread's workspace (out_keys / out_ids, rows of k_eff entries, sentinel
 // padded).  Queries are processed in chunks so the key matrix (nq_chunk x n
 // u32) stays within a fixed HBM budget (OVB_KEYS_BUDGET_MB, default 2048).
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 
@@ -128,9 +129,82 @@ uint64_t default_candidate_count(uint64_t k, uint64_t space) {
   return c < space ? c : space;
 }
 
+// Batched full scans use the split-BF16 tensor-core scan (with the exact FP64
+// rescoring below) from 64 queries on eligible shapes; OVB_RANK_TC=0/1 forces.
+bool use_rank_tc(const Index& rq, uint64_t nq) {
+  const char* e = getenv("OVB_RANK_TC");
+  if (!rank_tc_eligible(rq.dim, rq.bits)) return false;
+  if (e && e[0] == '0') return false;
+  if (e && e[0] == '1') return true;
+  return nq >= 64 && rq.n >= 4096;
+}
+
+uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t nq, uint64_t k, bool exact,
+                                     Workspace& w, cudaStream_t st) {
+  require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "search_asymmetric");
+  if (!rank_tc_eligible(rq.dim, rq.bits))
+    fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "split-BF16 scan needs dim to be a multiple of 64");
+  const uint64_t n = rq.n;
+  const uint32_t ke = (uint32_t)(k < n ? k : n);
+  if (!ke || !nq) return ke;
+  const uint32_t dim = rq.dim, bits = rq.bits;
+  const float* qu = normalised(w, d_q, nq, dim, st);
+  const float inv_norm = inv_rankquant_norm(dim, bits);
+  const float bound = split_error_bound(dim, bits, inv_norm);
+  uint16_t* qs = (uint16_t*)w.q_split.ensure(nq * 2 * dim * 2);
+  float* l1 = (float*)w.q_l1.ensure(nq * 4);
+  launch_split_queries(qu, nq, dim, qs, l1, st);
+  uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
+  uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
+  uint64_t qc = keys_budget() / (n * 4);
+  if (qc < 1) qc = 1;
+  if (qc > nq) qc = nq;
+  uint32_t* keys = (uint32_t*)w.keys.ensure(qc * n * 4);
+  uint32_t* flag = (uint32_t*)w.f_flag.ensure(4);
+  uint32_t* flag_h = (uint32_t*)w.f_flag_host.ensure(4);
+  const uint32_t id_bits = bits_for(n - 1);
+  for (uint64_t q0 = 0; q0 < nq; q0 += qc) {
+    const uint64_t qn = nq - q0 < qc ? nq - q0 : qc;
+    launch_rank_scan_tc(rq.codes.as<uint8_t>(), n, dim, bits, qs + q0 * 2 * dim, qn, inv_norm, keys, n, 0,
+                        w.tc_err_word(st), st);
+    w.mark(st, 2);
+    if (!exact) {
+      select_rows(w, keys, nullptr, nullptr, n, n, qn, ke, 32, id_bits, ok + q0 * ke, oi + q0 * ke, st);
+      w.mark(st, 3);
+      continue;
+    }
+    // candidates: the top kp by split score, kp grown until the kp-th is more
+    // than twice the bound below the k-th, so every doc whose exact score can
+    // reach the exact top-k is a candidate; the key matrix is reused
+    uint64_t kp = std::max<uint64_t>(2ull * ke, ke + 64ull);
+    for (;;) {
+      if (kp > n) kp = n;
+      uint32_t* tk = (uint32_t*)w.thr_keys.ensure(qn * kp * 4);
+      uint32_t* ti = (uint32_t*)w.thr_ids.ensure(qn * kp * 4);
+      select_rows(w, keys, nullptr, nullptr, n, n, qn, (uint32_t)kp, 32, id_bits, tk, ti, st);
+      if (kp == n) break;
+      OVB_CUDA(cudaMemsetAsync(flag, 0, 4, st));
+      launch_split_margin(tk, qn, (uint32_t)kp, ke, l1 + q0, bound, flag, st);
+      OVB_CUDA(cudaMemcpyAsync(flag_h, flag, 4, cudaMemcpyDeviceToHost, st));
+      OVB_CUDA(cudaStreamSynchronize(st));
+      if (!*flag_h) break;
+      kp *= 4;
+    }
+    uint64_t* off = (uint64_t*)w.off.ensure((qn + 1) * 8);
+    launch_uniform_offsets(off, qn, (uint32_t)kp, st);
+    uint32_t* k2 = (uint32_t*)w.keys2.ensure(qn * kp * 4);
+    const uint32_t* ti = w.thr_ids.as<uint32_t>();
+    launch_asym_subset(rq.codes.as<uint8_t>(), dim, bits, qu + q0 * dim, qn, off, ti, kp, inv_norm, k2, st);
+    select_rows(w, k2, ti, off, 0, 0, qn, ke, 32, id_bits, ok + q0 * ke, oi + q0 * ke, st);
+    w.mark(st, 3);
+  }
+  return ke;
+}
+
 uint32_t engine_rankquant_full(const Index& rq, const float* d_q, uint64_t nq, uint64_t k,
                                Workspace& w, cudaStream_t st) {
   require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "search_asymmetric");
+  if (use_rank_tc(rq, nq)) return engine_rankquant_full_split(rq, d_q, nq, k, true, w, st);
   const uint32_t ke = (uint32_t)(k < rq.n ? k : rq.n);
   if (!ke || !nq) return ke;
   const float* qu = normalised(w, d_q, nq, rq.dim, st);

@@ -100,6 +100,8 @@ struct Workspace {
   // FastScan threshold filter: sample key matrix, per-query thresholds,
   // kept (key, id) rows, their counts and the failure flag
   DevBuf smp_keys, thr_keys, thr_ids, f_keys, f_ids, f_cnt, f_flag;
+  // split-BF16 rank scan: [hi; lo] query rows and |q|_1
+  DevBuf q_split, q_l1;
   HostBuf pinned, f_flag_host;
   // error word of the tensor-core kernels (zeroed once; checked by host APIs)
   DevBuf tc_err;
@@ -132,6 +134,11 @@ void ensure_device();
 // pipelines on device pointers (engine.cpp); return the effective k
 uint32_t engine_rankquant_full(const Index& rq, const float* d_q, uint64_t nq, uint64_t k,
                                Workspace& w, cudaStream_t st);
+// Full search scored by the split-BF16 tensor-core scan; exact = true rescores
+// the candidates within the error bound in FP64 (the same top-k as the exact
+// path), false returns the split-BF16 scores and their top-k.
+uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t nq, uint64_t k, bool exact,
+                                     Workspace& w, cudaStream_t st);
 uint32_t engine_rankquant_subset(const Index& rq, const float* d_q, uint64_t nq,
                                  const uint64_t* d_off, const uint32_t* d_cands, uint64_t max_row,
                                  uint64_t k, Workspace& w, cudaStream_t st);

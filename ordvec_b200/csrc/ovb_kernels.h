@@ -82,6 +82,21 @@ void launch_filter_check(const uint32_t* cnt, uint64_t nq, uint32_t need, uint32
 void launch_fastscan_relayout(const uint8_t* ref_blocks, uint64_t n, uint32_t pairs,
                               uint32_t pairs_pad, uint8_t* dev_blocks, cudaStream_t stream);
 
+// ---- K4-TC split-BF16 asymmetric scan on tcgen05 (scan_rank_tc.cu) -------------
+bool rank_tc_eligible(uint32_t dim, uint32_t bits);
+// |split score - exact score| <= split_error_bound(...) * |q_unit|_1
+float split_error_bound(uint32_t dim, uint32_t bits, float inv_norm);
+// q_unit rows -> [2 nq x dim] bf16 (row 2i = hi, 2i+1 = lo) and |q|_1 per row
+void launch_split_queries(const float* q_unit, uint64_t nq, uint32_t dim, void* out_bf16, float* l1,
+                          cudaStream_t stream);
+// keys[q][doc] (ld) = desc key of the split-BF16 score; q_per_tile 0 = default
+void launch_rank_scan_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_t bits, const void* q_split,
+                         uint64_t nq, float inv_norm, uint32_t* keys, uint64_t ld, uint32_t q_per_tile, uint32_t* err,
+                         cudaStream_t stream);
+// flag |= 1 if some row's kp-th key is not below its k-th minus twice the bound
+void launch_split_margin(const uint32_t* sel_keys, uint64_t nq, uint32_t kp, uint32_t k, const float* l1,
+                         float bound_per_l1, uint32_t* flag, cudaStream_t stream);
+
 // ---- K4/K5 asymmetric RankQuant scoring (scan_asym.cu) ---------------------------
 void launch_asym_scan(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_t bits,
                       const float* q_unit, uint64_t nq, float inv_norm, uint32_t* keys,

@@ -287,6 +287,44 @@ def test_rankquant_search_matches_fp64(orc, dim, bits):
             check_float_topk(res.indices_for_query(qi), res.scores_for_query(qi), np.arange(n), s64, k)
 
 
+def _split_bound(dim, bits, q):
+    """The split-BF16 error bound the library states (scan_rank_tc.cu)."""
+    qn = np.asarray(q, np.float64)
+    qn = qn / np.sqrt((qn * qn).sum())
+    inv_norm = 1.0 / np.sqrt(dim * ((4.0 ** bits - 1.0) / 12.0))
+    cmax = (2 ** bits - 1) / 2
+    return inv_norm * cmax * (2 * dim * 2.0 ** -24 + 2.0 ** -16) * 1.05 * np.abs(qn).sum()
+
+
+@pytest.mark.parametrize("dim,bits,n", [(1024, 2, 20_000), (1024, 1, 9_000), (768, 4, 7_000), (128, 2, 5_000)])
+def test_split_bf16_rank_scan(orc, monkeypatch, dim, bits, n):
+    """Tensor-core split-BF16 full search: the exact form (default for >= 64
+    queries) meets the FP64 bar; the raw split scores stay within the stated
+    error bound; forcing the path on and off changes nothing."""
+    nq = 80
+    docs = ob.synth_docs(13 + bits, n, dim)
+    queries, _ = ob.synth_queries(13 + bits, n, nq, dim)
+    rq = ob.RankQuant(dim, bits)
+    rq.add(docs)
+    packed = orc.rankquant_encode(docs, dim, bits)
+    for k in (10, 100):
+        res = rq.search_asymmetric(queries, k)
+        raw = rq.search_asymmetric_split(queries, k, exact=False)
+        worst = 0.0
+        for qi in (0, 1, 41, 79):
+            s64 = orc.rq_scores_f64(packed, n, dim, bits, queries[qi])
+            check_float_topk(res.indices_for_query(qi), res.scores_for_query(qi), np.arange(n), s64, k)
+            err = np.abs(raw.scores_for_query(qi).astype(np.float64) - s64[raw.indices_for_query(qi)])
+            worst = max(worst, err.max())
+            assert err.max() <= _split_bound(dim, bits, queries[qi]), (qi, err.max())
+        print(f"split-BF16 dim {dim} b{bits} k {k}: max |split - fp64| = {worst:.3e}")
+    monkeypatch.setenv("OVB_RANK_TC", "1")
+    a = rq.search_asymmetric(queries[:5], 10)
+    monkeypatch.setenv("OVB_RANK_TC", "0")
+    b = rq.search_asymmetric(queries[:5], 10)
+    assert np.array_equal(a.indices, b.indices)
+
+
 def test_rankquant_large_k_uses_global_select(orc):
     dim, bits, n = 128, 2, 9000
     docs = ob.synth_docs(5, n, dim)
