@@ -186,6 +186,28 @@ ordvec_status_t ovb_rankquant_search(const ordvec_index_t *rq, const float *quer
 ordvec_status_t ovb_rankquant_search_split(const ordvec_index_t *rq, const float *queries,
                                            uint64_t nq, uint64_t k, uint32_t exact,
                                            float *scores, int64_t *ids);
+/* Mixed batch (no counterpart in the reference): query i is searched in full
+ * in indices[index_of_query[i]] (RankQuant indices of one dim, e.g. one
+ * corpus at bits 1, 2 and 4) for its own k_of_query[i] <= k_max, all in one
+ * call.  Output rows hold k_max entries: row i's first min(k_of_query[i], n)
+ * are its top-k (score desc, id asc, the results ovb_rankquant_search gives),
+ * the rest (-inf, -1).  Queries are grouped by index; each group on the
+ * split-BF16 tensor-core path runs through a plan cached per (index, group
+ * size, k): its first call tunes the scan's tile shape and records the
+ * pipeline as a CUDA graph, later calls replay it (falling back to the exact
+ * pipeline when the fixed candidate count is too small for a query).
+ * OVB_MIXED_GRAPH=0 disables the plans. */
+ordvec_status_t ovb_rankquant_search_mixed(const ordvec_index_t *const *indices,
+                                           uint32_t n_indices, const uint32_t *index_of_query,
+                                           const uint32_t *k_of_query, const float *queries,
+                                           uint64_t nq, uint64_t k_max, float *scores,
+                                           int64_t *ids);
+/* The cached plan of (rq, group size nq, k): the tuned queries per tile of its
+ * scan, its candidate count and how many times its graph was replayed.
+ * BAD_ARGUMENT when no plan exists. */
+ordvec_status_t ovb_mixed_plan_info(const ordvec_index_t *rq, uint64_t nq, uint64_t k,
+                                    uint32_t *q_per_tile, uint64_t *candidates,
+                                    uint64_t *replays);
 /* RankQuant::search_asymmetric_subset_batched_serial_into (src/quant.rs:1336-1394):
  * CSR candidates (offsets[nq+1]), output nq x min(k, n). */
 ordvec_status_t ovb_rankquant_search_subset(const ordvec_index_t *rq, const float *queries,

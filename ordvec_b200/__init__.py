@@ -7,10 +7,10 @@ from ._lib import LIB_PATH, OrdvecError, lib
 from .api import (Bitmap, CandidateBatch, MultiBucketBitmap, RankQuant, RankQuantFastscan,
                   SearchResults, Server, SignBitmap, Ticket, TwoStageCandidatePolicy, last_launch_count, load,
                   set_device, synth_docs, synth_queries, two_stage_profile, two_stage_search,
-                  two_stage_search_device)
+                  two_stage_search_device, search_mixed, mixed_plan_info)
 
 __all__ = [
     "Bitmap", "CandidateBatch", "MultiBucketBitmap", "OrdvecError", "RankQuant", "RankQuantFastscan",
     "SearchResults", "SignBitmap", "TwoStageCandidatePolicy", "LIB_PATH", "last_launch_count", "lib",
-    "load", "synth_docs", "synth_queries", "two_stage_search", "Server", "Ticket",
+    "load", "synth_docs", "synth_queries", "two_stage_search", "Server", "Ticket", "search_mixed", "mixed_plan_info",
 ]

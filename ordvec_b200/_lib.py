@@ -117,6 +117,8 @@ SIGNATURES = {
     "ovb_synth_docs": (S, [U64, U64, U64, U32, F, P]),
     "ovb_synth_queries": (S, [U64, U64, U64, U32, F, F, P, P]),
     "ovb_rankquant_search_split": (S, [P, P, U64, U64, U32, P, P]),
+    "ovb_rankquant_search_mixed": (S, [P, U32, P, P, P, U64, U64, P, P]),
+    "ovb_mixed_plan_info": (S, [P, U64, U64, P, P, P]),
     "ovb_server_new": (S, [P, P]),
     "ovb_server_add_route": (S, [P, P, P, P]),
     "ovb_server_submit": (S, [P, U32, P, U64, U64, U64, P]),

@@ -415,6 +415,36 @@ def two_stage_search(rq: RankQuant, stage1: _Index, queries, m: int, k: int) -> 
     return SearchResults(s[: nq * ke], i[: nq * ke], nq, ke)
 
 
+def search_mixed(indices: Sequence[RankQuant], index_of_query, k_of_query, queries) -> SearchResults:
+    """One call for queries with their own index and k (ovb_rankquant_search_mixed):
+    row i holds query i's top-k_of_query[i] in indices[index_of_query[i]],
+    padded to max(k_of_query) with (-inf, -1)."""
+    if not indices:
+        raise OrdvecError(2, "indices must not be empty")
+    dim = indices[0].dim
+    q = _rows(queries, dim)
+    nq = q.size // dim
+    sel = np.ascontiguousarray(index_of_query, np.uint32)
+    ks = np.ascontiguousarray(k_of_query, np.uint32)
+    if sel.size != nq or ks.size != nq:
+        raise OrdvecError(2, "index_of_query and k_of_query need one entry per query")
+    k_max = int(ks.max()) if nq else 0
+    handles = (C.c_void_p * len(indices))(*[ix.handle.value if hasattr(ix.handle, "value") else ix.handle
+                                            for ix in indices])
+    s = np.empty(max(nq * k_max, 1), np.float32)
+    i = np.empty(max(nq * k_max, 1), np.int64)
+    check(lib().ovb_rankquant_search_mixed(handles, len(indices), _ptr(sel), _ptr(ks), _ptr(q), nq, k_max,
+                                           _ptr(s), _ptr(i)))
+    return SearchResults(s[: nq * k_max], i[: nq * k_max], nq, k_max)
+
+
+def mixed_plan_info(rq: RankQuant, nq: int, k: int) -> dict:
+    """Tuned tile (queries per tile), candidate count and graph replays of a plan."""
+    qpt, kp, rep = C.c_uint32(), C.c_uint64(), C.c_uint64()
+    check(lib().ovb_mixed_plan_info(rq.handle, nq, k, C.byref(qpt), C.byref(kp), C.byref(rep)))
+    return {"q_per_tile": qpt.value, "candidates": kp.value, "replays": rep.value}
+
+
 class Server:
     """Serving loop over device-resident indices (ovb_server_*): requests are
     queued, batched with other pending requests of the same route, k and m

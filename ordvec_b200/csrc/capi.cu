@@ -330,6 +330,7 @@ void ordvec_index_free(ordvec_index_t* index) {
   if (!index) return;
   Index* ix = (Index*)index;
   if (ix->magic != kIndexMagic) return;
+  mixed_forget_index(ix);
   ix->magic = 0;
   delete ix;
 }
@@ -505,6 +506,7 @@ ordvec_status_t ovb_multibucket_new(uint32_t dim, uint32_t bits, ordvec_index_t*
 ordvec_status_t ovb_index_add(ordvec_index_t* index, const float* vectors, uint64_t n) {
   return boundary([&] {
     Index& ix = as_index_mut(index);
+    mixed_forget_index(&ix);  // cached mixed-batch plans describe the old rows
     if (n && !vectors) fail(ORDVEC_STATUS_NULL_POINTER, "vectors pointer is NULL");
     if (!n) return;
     if (!all_finite(vectors, n * ix.dim))
@@ -538,6 +540,7 @@ ordvec_status_t ovb_index_add(ordvec_index_t* index, const float* vectors, uint6
 ordvec_status_t ovb_index_add_device(ordvec_index_t* index, const float* d_vectors, uint64_t n) {
   return boundary([&] {
     Index& ix = as_index_mut(index);
+    mixed_forget_index(&ix);  // cached mixed-batch plans describe the old rows
     if (n && !d_vectors) fail(ORDVEC_STATUS_NULL_POINTER, "vectors pointer is NULL");
     if (!n) return;
     Workspace& w = workspace();

@@ -121,6 +121,8 @@ void require_kind(const Index& ix, uint32_t kind, const char* what) {
 
 }  // namespace
 
+uint64_t engine_keys_budget() { return keys_budget(); }
+
 uint64_t default_candidate_count(uint64_t k, uint64_t space) {
   // TwoStageCandidatePolicy::default() (src/quant.rs:242-262): min 256, k*32.
   if (k == 0 || space == 0) return 0;
@@ -140,7 +142,7 @@ bool use_rank_tc(const Index& rq, uint64_t nq) {
 }
 
 uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t nq, uint64_t k, bool exact,
-                                     Workspace& w, cudaStream_t st) {
+                                     Workspace& w, cudaStream_t st, uint32_t q_per_tile) {
   require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "search_asymmetric");
   if (!rank_tc_eligible(rq.dim, rq.bits))
     fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "split-BF16 scan needs dim to be a multiple of 64");
@@ -163,10 +165,11 @@ uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t
   uint32_t* flag = (uint32_t*)w.f_flag.ensure(4);
   uint32_t* flag_h = (uint32_t*)w.f_flag_host.ensure(4);
   const uint32_t id_bits = bits_for(n - 1);
+  w.split_kp = 0;
   for (uint64_t q0 = 0; q0 < nq; q0 += qc) {
     const uint64_t qn = nq - q0 < qc ? nq - q0 : qc;
-    launch_rank_scan_tc(rq.codes.as<uint8_t>(), n, dim, bits, qs + q0 * 2 * dim, qn, inv_norm, keys, n, 0,
-                        w.tc_err_word(st), st);
+    launch_rank_scan_tc(rq.codes.as<uint8_t>(), n, dim, bits, qs + q0 * 2 * dim, qn, inv_norm, keys, n,
+                        q_per_tile, w.tc_err_word(st), st);
     w.mark(st, 2);
     if (!exact) {
       select_rows(w, keys, nullptr, nullptr, n, n, qn, ke, 32, id_bits, ok + q0 * ke, oi + q0 * ke, st);
@@ -190,6 +193,7 @@ uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t
       if (!*flag_h) break;
       kp *= 4;
     }
+    w.split_kp = std::max<uint64_t>(w.split_kp, kp);
     uint64_t* off = (uint64_t*)w.off.ensure((qn + 1) * 8);
     launch_uniform_offsets(off, qn, (uint32_t)kp, st);
     uint32_t* k2 = (uint32_t*)w.keys2.ensure(qn * kp * 4);
@@ -198,6 +202,38 @@ uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t
     select_rows(w, k2, ti, off, 0, 0, qn, ke, 32, id_bits, ok + q0 * ke, oi + q0 * ke, st);
     w.mark(st, 3);
   }
+  return ke;
+}
+
+uint32_t engine_rankquant_split_fixed(const Index& rq, const float* d_q, uint64_t nq, uint64_t k, uint64_t kp,
+                                      uint32_t q_per_tile, uint32_t* d_flag, Workspace& w, cudaStream_t st) {
+  require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "search_asymmetric");
+  const uint64_t n = rq.n;
+  const uint32_t ke = (uint32_t)(k < n ? k : n);
+  if (!ke || !nq) return ke;
+  if (!rank_tc_eligible(rq.dim, rq.bits) || nq * n * 4 > keys_budget())
+    fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "fixed split search: shape outside the single-chunk form");
+  if (kp > n) kp = n;
+  if (kp < ke) kp = ke;
+  const uint32_t dim = rq.dim, bits = rq.bits, id_bits = bits_for(n - 1);
+  const float* qu = normalised(w, d_q, nq, dim, st);
+  const float inv_norm = inv_rankquant_norm(dim, bits);
+  uint16_t* qs = (uint16_t*)w.q_split.ensure(nq * 2 * dim * 2);
+  float* l1 = (float*)w.q_l1.ensure(nq * 4);
+  launch_split_queries(qu, nq, dim, qs, l1, st);
+  uint32_t* keys = (uint32_t*)w.keys.ensure(nq * n * 4);
+  launch_rank_scan_tc(rq.codes.as<uint8_t>(), n, dim, bits, qs, nq, inv_norm, keys, n, q_per_tile,
+                      w.tc_err_word(st), st);
+  uint32_t* tk = (uint32_t*)w.thr_keys.ensure(nq * kp * 4);
+  uint32_t* ti = (uint32_t*)w.thr_ids.ensure(nq * kp * 4);
+  select_rows(w, keys, nullptr, nullptr, n, n, nq, (uint32_t)kp, 32, id_bits, tk, ti, st);
+  if (kp < n) launch_split_margin(tk, nq, (uint32_t)kp, ke, l1, split_error_bound(dim, bits, inv_norm), d_flag, st);
+  uint64_t* off = (uint64_t*)w.off.ensure((nq + 1) * 8);
+  launch_uniform_offsets(off, nq, (uint32_t)kp, st);
+  uint32_t* k2 = (uint32_t*)w.keys2.ensure(nq * kp * 4);
+  launch_asym_subset(rq.codes.as<uint8_t>(), dim, bits, qu, nq, off, ti, kp, inv_norm, k2, st);
+  select_rows(w, k2, ti, off, 0, 0, nq, ke, 32, id_bits, (uint32_t*)w.out_keys.ensure(nq * ke * 4),
+              (uint32_t*)w.out_ids.ensure(nq * ke * 4), st);
   return ke;
 }
 

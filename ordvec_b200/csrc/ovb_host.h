@@ -102,6 +102,7 @@ struct Workspace {
   DevBuf smp_keys, thr_keys, thr_ids, f_keys, f_ids, f_cnt, f_flag;
   // split-BF16 rank scan: [hi; lo] query rows and |q|_1
   DevBuf q_split, q_l1;
+  uint64_t split_kp = 0;  // largest candidate count the last exact split search settled on
   HostBuf pinned, f_flag_host;
   // error word of the tensor-core kernels (zeroed once; checked by host APIs)
   DevBuf tc_err;
@@ -138,7 +139,13 @@ uint32_t engine_rankquant_full(const Index& rq, const float* d_q, uint64_t nq, u
 // the candidates within the error bound in FP64 (the same top-k as the exact
 // path), false returns the split-BF16 scores and their top-k.
 uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t nq, uint64_t k, bool exact,
-                                     Workspace& w, cudaStream_t st);
+                                     Workspace& w, cudaStream_t st, uint32_t q_per_tile = 0);
+// The exact split search with a fixed candidate count kp and no host
+// synchronisation (capturable once the workspace is sized; nq * n * 4 bytes of
+// keys must fit the key budget): *d_flag |= 1 (caller-zeroed) when the margin
+// test fails for some query, i.e. when kp was too small for an exact result.
+uint32_t engine_rankquant_split_fixed(const Index& rq, const float* d_q, uint64_t nq, uint64_t k, uint64_t kp,
+                                      uint32_t q_per_tile, uint32_t* d_flag, Workspace& w, cudaStream_t st);
 uint32_t engine_rankquant_subset(const Index& rq, const float* d_q, uint64_t nq,
                                  const uint64_t* d_off, const uint32_t* d_cands, uint64_t max_row,
                                  uint64_t k, Workspace& w, cudaStream_t st);
@@ -152,6 +159,12 @@ uint32_t engine_fastscan_full(const Index& fs, const float* d_q, uint64_t nq, ui
 uint32_t engine_two_stage(const Index& rq, const Index& s1, const float* d_q, uint64_t nq,
                           uint64_t m, uint64_t k, Workspace& w, cudaStream_t st);
 uint64_t default_candidate_count(uint64_t k, uint64_t space);
+uint64_t engine_keys_budget();  // bytes a key matrix chunk may take
+
+// mixed batches (mixed.cu): drop the cached plans of an index that is freed or
+// grows; plan facts for tests and tools
+void mixed_forget_index(const Index* ix);
+bool mixed_plan_info(const Index& ix, uint64_t nq, uint64_t k, uint32_t* qpt, uint64_t* kp, uint64_t* replays);
 
 // persistence (persist.cpp)
 std::unique_ptr<Index> load_index_file(const char* path, bool v1_only);
