@@ -154,6 +154,50 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------- mixed batch
+def mixed_run(ob, nq: int, steps: int):
+    """The mixed-k / mixed-bits batch configuration: N=1,000,000 synthetic docs,
+    dim 1024, RankQuant indices at bits 1, 2 and 4 over the same corpus, nq
+    queries each with its own bits and k in {10, 50, 100}, one call per step
+    (ovb_rankquant_search_mixed: split-BF16 tensor-core scan + exact FP64
+    rescoring, plans with autotuned tiles and CUDA-graph replay).  Host
+    buffers in and out; wall time per call after the first (tuning) call."""
+    n, dim, seed = 1_000_000, 1024, 0x0DD5EED3
+    docs = ob.synth_docs(seed, n, dim)
+    queries, _ = ob.synth_queries(seed + 1, n, nq, dim)
+    indices = []
+    for bits in (1, 2, 4):
+        rq = ob.RankQuant(dim, bits)
+        rq.add(docs)
+        indices.append(rq)
+    del docs
+    rng = np.random.default_rng(seed)
+    sel = rng.integers(0, 3, nq).astype(np.uint32)
+    ks = rng.choice([10, 50, 100], nq).astype(np.uint32)
+    t0 = time.perf_counter()
+    first = ob.search_mixed(indices, sel, ks, queries)
+    first_s = time.perf_counter() - t0
+    reps = max(1, min(steps, 5))
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        res = ob.search_mixed(indices, sel, ks, queries)
+        times.append(time.perf_counter() - t0)
+    same = bool(np.array_equal(res.indices, first.indices))
+    plans = []
+    for j, rq in enumerate(indices):
+        rows = np.flatnonzero(sel == j)
+        if rows.size:
+            info = ob.mixed_plan_info(rq, rows.size, int(ks[rows].max()))
+            plans.append({"bits": (1, 2, 4)[j], "queries": int(rows.size), **info})
+    sec = float(np.median(times))
+    flops = 2 * 2 * nq * n * dim  # hi and lo products, multiply + add
+    return {"workload": f"N={n} dim={dim} bits {{1,2,4}} k {{10,50,100}}, {nq} mixed queries per call",
+            "qps": nq / sec, "s_per_call": sec, "first_call_s": first_s, "calls": reps,
+            "split_bf16_tflops_effective": flops / sec / 1e12, "identical_across_calls": same, "plans": plans,
+            "form": "host buffers; split-BF16 tcgen05 scan + exact FP64 rescoring; CUDA-graph replay"}
+
+
 # ------------------------------------------------------------------ serving
 def serving_run(ob, rq, fs, queries, batched_ids, seconds: float, rate_qps: float):
     """The serving loop on this workload's route: seeded Poisson request
@@ -221,6 +265,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-rate", type=float, default=150_000.0, help="offered queries/s")
+    ap.add_argument("--mixed-queries", type=int, default=0,
+                    help="also run the mixed-k/bits batch (N=1M, dim 1024) with this many queries; 0 = skip")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -377,6 +423,7 @@ def main():
                   "p99_ms": float(np.percentile(plain_ms, 99)), "queries": P, "launches_per_query": plain_launches,
                   "identical_top10_vs_batched": identical, "batched_over_plain": value / world / plain_qps},
         "serving": serving,
+        "mixed_batch": mixed_run(ob, args.mixed_queries, args.steps) if args.mixed_queries > 0 else None,
         "stages_ms": dict(zip(STAGES, stages)),
         "stages_ms_plain": dict(zip(STAGES, stages1)),
         "scan_gbs_effective": NQ * ref_code_bytes / (stages[2] * 1e-3) / 1e9,
