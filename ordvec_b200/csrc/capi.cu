@@ -670,7 +670,11 @@ static void top_m_host(const Index& ix, const float* queries, uint64_t nq, uint6
   Workspace& w = workspace();
   const float* d_q = upload_queries(w, queries, nq, ix.dim, true);
   const float* d_w = nullptr;
-  if (weights) {
+  bool identity = weights != nullptr;  // identity weights take the integer (tensor-core) path
+  for (uint32_t a = 0; identity && a < ix.nb(); a++)
+    for (uint32_t b = 0; b < ix.nb(); b++)
+      if (weights[a * ix.nb() + b] != (a == b ? 1.0f : 0.0f)) identity = false;
+  if (weights && !identity) {
     float* dw = (float*)w.weights.ensure(ix.nb() * ix.nb() * 4);
     OVB_CUDA(cudaMemcpyAsync(dw, weights, ix.nb() * ix.nb() * 4, cudaMemcpyHostToDevice, w.stream));
     d_w = dw;

@@ -115,6 +115,96 @@ bool filter_plan(uint64_t n, uint32_t m, FilterPlan& p) {
   return true;
 }
 
+// Stage-1 top-m rows through the sampled threshold filter.
+//   sample(q0, qn, keys)                 sample keys, rows of fp.n_s
+//   filter(q0, qn, thr, pos, cnt, fk, fi) filtering scan; thr / pos: the r-th
+//                                        sample key and its sample position,
+//                                        row stride fp.r
+//   dense(qa, qn)                        rows [qa, qa + qn) through the full key matrix
+template <class Sample, class Filter, class Dense>
+void filtered_select(Workspace& w, uint64_t n, uint64_t nq, uint32_t me, const FilterPlan& fp, uint32_t key_bits,
+                     uint32_t* sk, uint32_t* si, cudaStream_t st, Sample&& sample, Filter&& filter,
+                     Dense&& dense) {
+  const uint64_t per_q = fp.n_s * 4 + (uint64_t)fp.r * 8 + (uint64_t)fp.cap * 8 + 4;
+  uint64_t qc = keys_budget() / per_q;
+  if (qc < 1) qc = 1;
+  if (qc > nq) qc = nq;
+  uint32_t* smp = (uint32_t*)w.smp_keys.ensure(qc * fp.n_s * 4);
+  uint32_t* tk = (uint32_t*)w.thr_keys.ensure(qc * fp.r * 4);
+  uint32_t* ti = (uint32_t*)w.thr_ids.ensure(qc * fp.r * 4);
+  uint32_t* fk = (uint32_t*)w.f_keys.ensure(qc * fp.cap * 4);
+  uint32_t* fi = (uint32_t*)w.f_ids.ensure(qc * fp.cap * 4);
+  uint32_t* cnt = (uint32_t*)w.f_cnt.ensure(qc * 4);
+  uint32_t* flag = (uint32_t*)w.f_flag.ensure(4);
+  uint32_t* flag_h = (uint32_t*)w.f_flag_host.ensure(4);
+  for (uint64_t q0 = 0; q0 < nq; q0 += qc) {
+    const uint64_t qn = nq - q0 < qc ? nq - q0 : qc;
+    sample(q0, qn, smp);
+    select_rows(w, smp, nullptr, nullptr, fp.n_s, fp.n_s, qn, fp.r, key_bits, bits_for(fp.n_s - 1), tk, ti, st);
+    w.mark(st, 6);
+    OVB_CUDA(cudaMemsetAsync(cnt, 0, qn * 4, st));
+    OVB_CUDA(cudaMemsetAsync(flag, 0, 4, st));
+    filter(q0, qn, tk + (fp.r - 1), ti + (fp.r - 1), cnt, fk, fi);
+    launch_filter_check(cnt, qn, me, fp.cap, flag, st);
+    OVB_CUDA(cudaMemcpyAsync(flag_h, flag, 4, cudaMemcpyDeviceToHost, st));
+    OVB_CUDA(cudaStreamSynchronize(st));
+    if (*flag_h) {
+      dense(q0, qn);
+      continue;
+    }
+    w.mark(st, 2);
+    select_rows(w, fk, fi, nullptr, fp.cap, fp.cap, qn, me, key_bits, bits_for(n - 1), sk + q0 * me, si + q0 * me,
+                st, cnt);
+    w.mark(st, 3);
+  }
+}
+
+// Tensor-core overlap scan for constant-weight bitmaps and identity-weight
+// multi-bucket bitmaps, batches of at least 32 queries; OVB_BITMAP_TC=0/1 forces.
+bool use_bitmap_tc(uint64_t nq) {
+  const char* e = getenv("OVB_BITMAP_TC");
+  if (e && e[0] == '0') return false;
+  if (e && e[0] == '1') return true;
+  return nq >= 32;
+}
+
+// Stage-1 top-m of a bitmap-family index on the tensor cores: key_kind 0 for a
+// constant-weight bitmap, 1 for a multi-bucket bitmap with identity weights;
+// qb = query words (qpv per query).
+void bitmap_tc_candidates(const Index& s1, const uint64_t* qb, uint32_t qpv, uint32_t key_kind, uint32_t key_bits,
+                          uint64_t nq, uint32_t me, uint32_t* sk, uint32_t* si, Workspace& w, cudaStream_t st) {
+  const uint64_t n = s1.n;
+  const uint64_t row = (uint64_t)bitmap_tc_kblocks(qpv) * 128;
+  uint8_t* qx = (uint8_t*)w.lut.ensure(nq * row);
+  launch_bitmap_tc_query(qb, nq, qpv, qx, st);
+  const uint64_t* words = s1.codes.as<uint64_t>();
+  uint32_t* err = w.tc_err_word(st);
+  auto dense = [&](uint64_t qa, uint64_t qn) {
+    full_scan_select(w, qn, n, me, key_bits, sk + qa * me, si + qa * me, st,
+                     [&](uint64_t q0, uint64_t qm, uint32_t* keys) {
+                       launch_bitmap_scan_tc(words, n, qpv, key_kind, s1.n_top, qx + (qa + q0) * row, qm, 1, keys, n,
+                                             err, st);
+                     });
+  };
+  FilterPlan fp;
+  if (!filter_plan(n, me, fp)) {
+    w.mark(st, 6);  // no sampling stage
+    dense(0, nq);
+    return;
+  }
+  filtered_select(
+      w, n, nq, me, fp, key_bits, sk, si, st,
+      [&](uint64_t q0, uint64_t qn, uint32_t* smp) {
+        launch_bitmap_scan_tc(words, n, qpv, key_kind, s1.n_top, qx + q0 * row, qn, fp.stride, smp, fp.n_s, err, st);
+      },
+      [&](uint64_t q0, uint64_t qn, const uint32_t* thr, const uint32_t* pos, uint32_t* cnt, uint32_t* fk,
+          uint32_t* fi) {
+        launch_bitmap_filter_tc(words, n, qpv, key_kind, s1.n_top, qx + q0 * row, qn, thr, pos, fp.stride, fp.r, cnt,
+                                fp.cap, fk, fi, err, st);
+      },
+      dense);
+}
+
 void require_kind(const Index& ix, uint32_t kind, const char* what) {
   if (ix.kind != kind) fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, std::string(what) + ": wrong index kind");
 }
@@ -290,8 +380,12 @@ uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint6
       else
         launch_bitmap_query(d_q, nq, s1.dim, s1.n_top, qb, st);
       w.mark(st, 1);
-      w.mark(st, 6);  // no sampling stage
       const uint32_t key_bits = bits_for(mode == 0 ? s1.dim : s1.n_top);
+      if (mode == 1 && use_bitmap_tc(nq)) {
+        bitmap_tc_candidates(s1, qb, s1.qpv(), 0, key_bits, nq, me, sk, si, w, st);
+        break;
+      }
+      w.mark(st, 6);  // no sampling stage
       full_scan_select(w, nq, n, me, key_bits, sk, si, st, [&](uint64_t q0, uint64_t qn, uint32_t* keys) {
         launch_popc_scan(mode, s1.codes.as<uint64_t>(), n, s1.qpv(), qb + q0 * s1.qpv(), qn, s1.n_top, keys,
                          n, st);
@@ -327,41 +421,19 @@ uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint6
         dense_rows(0, nq);
         break;
       }
-      const uint64_t per_q = fp.n_s * 4 + (uint64_t)fp.r * 8 + (uint64_t)fp.cap * 8 + 4;
-      uint64_t qc = keys_budget() / per_q;
-      if (qc < 1) qc = 1;
-      if (qc > nq) qc = nq;
-      uint32_t* smp = (uint32_t*)w.smp_keys.ensure(qc * fp.n_s * 4);
-      uint32_t* tk = (uint32_t*)w.thr_keys.ensure(qc * fp.r * 4);
-      uint32_t* ti = (uint32_t*)w.thr_ids.ensure(qc * fp.r * 4);
-      uint32_t* fk = (uint32_t*)w.f_keys.ensure(qc * fp.cap * 4);
-      uint32_t* fi = (uint32_t*)w.f_ids.ensure(qc * fp.cap * 4);
-      uint32_t* cnt = (uint32_t*)w.f_cnt.ensure(qc * 4);
-      uint32_t* flag = (uint32_t*)w.f_flag.ensure(4);
-      uint32_t* flag_h = (uint32_t*)w.f_flag_host.ensure(4);
       uint32_t* err = w.tc_err_word(st);
-      for (uint64_t q0 = 0; q0 < nq; q0 += qc) {
-        const uint64_t qn = nq - q0 < qc ? nq - q0 : qc;
-        launch_fastscan_scan_tc(codes, n, s1.pairs_pad, lut + q0 * lut_row, bias + q0, invq + q0, inv_norm, qn,
-                                fp.stride, smp, fp.n_s, err, st);
-        select_rows(w, smp, nullptr, nullptr, fp.n_s, fp.n_s, qn, fp.r, 32, bits_for(fp.n_s - 1), tk, ti, st);
-        w.mark(st, 6);
-        OVB_CUDA(cudaMemsetAsync(cnt, 0, qn * 4, st));
-        OVB_CUDA(cudaMemsetAsync(flag, 0, 4, st));
-        launch_fastscan_filter_tc(codes, n, s1.pairs_pad, lut + q0 * lut_row, bias + q0, invq + q0, inv_norm, qn,
-                                  tk + (fp.r - 1), fp.r, cnt, fp.cap, fk, fi, err, st);
-        launch_filter_check(cnt, qn, me, fp.cap, flag, st);
-        OVB_CUDA(cudaMemcpyAsync(flag_h, flag, 4, cudaMemcpyDeviceToHost, st));
-        OVB_CUDA(cudaStreamSynchronize(st));
-        if (*flag_h) {
-          dense_rows(q0, qn);
-          continue;
-        }
-        w.mark(st, 2);
-        select_rows(w, fk, fi, nullptr, fp.cap, fp.cap, qn, me, 32, bits_for(n - 1), sk + q0 * me, si + q0 * me, st,
-                    cnt);
-        w.mark(st, 3);
-      }
+      filtered_select(
+          w, n, nq, me, fp, 32, sk, si, st,
+          [&](uint64_t q0, uint64_t qn, uint32_t* smp) {
+            launch_fastscan_scan_tc(codes, n, s1.pairs_pad, lut + q0 * lut_row, bias + q0, invq + q0, inv_norm, qn,
+                                    fp.stride, smp, fp.n_s, err, st);
+          },
+          [&](uint64_t q0, uint64_t qn, const uint32_t* thr, const uint32_t*, uint32_t* cnt, uint32_t* fk,
+              uint32_t* fi) {
+            launch_fastscan_filter_tc(codes, n, s1.pairs_pad, lut + q0 * lut_row, bias + q0, invq + q0, inv_norm,
+                                      qn, thr, fp.r, cnt, fp.cap, fk, fi, err, st);
+          },
+          dense_rows);
       break;
     }
     case OVB_INDEX_KIND_MULTIBUCKET: {
@@ -369,6 +441,12 @@ uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint6
       uint64_t* qb = (uint64_t*)w.qbits.ensure(nq * nb * qpb * 8);
       launch_multibucket_query(d_q, nq, s1.dim, s1.bits, qb, st);
       w.mark(st, 1);
+      if (!d_weights && use_bitmap_tc(nq)) {
+        // identity weights: the f32 sum over (a, a) of popcount(Q_a AND D_a)
+        // is the integer overlap of the concatenated bucket rows (exact below 2^24)
+        bitmap_tc_candidates(s1, qb, nb * qpb, 1, 32, nq, me, sk, si, w, st);
+        break;
+      }
       w.mark(st, 6);  // no sampling stage
       const float* wts = d_weights;
       if (!wts) {  // diagonal weights (src/multi_bucket.rs:157-164)

@@ -73,6 +73,7 @@ struct TcSmem {
   float invq[kTcMaxN];
   uint32_t thr[kTcMaxN];
   uint32_t amin[kTcMaxN];  // filter: smallest passing accumulator, or kExactCompare
+  uint32_t tdoc[kTcMaxN];  // bitmap filter, tie level: last passing doc id
   uint64_t full_a[kTcStages];
   uint64_t full_b[kTcStages];
   uint64_t empty[kTcStages];
@@ -87,9 +88,13 @@ struct TcSmem {
 };
 
 struct TcArgs {
-  const uint8_t* blocks;
+  const uint8_t* blocks;  // FastScan device blocks, or bitmap rows (u64 words)
   uint64_t n;
-  uint32_t pairs_pad;
+  uint32_t pairs_pad;     // FastScan
+  uint32_t qpv;           // bitmap: u64 words per row
+  uint32_t n_top;         // bitmap: set bits per row (key = n_top - overlap)
+  uint32_t key_kind;      // bitmap: 0 key = n_top - acc, 1 key = desc_key((float)acc)
+  uint32_t n_kb;          // 128-byte K-blocks
   uint32_t block_stride;
   const float* bias;
   const float* invq;
@@ -101,6 +106,8 @@ struct TcArgs {
   uint64_t ld;
   // filter output
   const uint32_t* thr;
+  const uint32_t* thr_pos;  // bitmap: sample position of the threshold (tie bound), or null
+  uint32_t smp_stride;      // block stride of the sample the positions index
   uint64_t thr_stride;
   uint32_t* cnt;
   uint32_t cap;
@@ -170,6 +177,28 @@ __device__ uint32_t filter_amin(float bias, float invq, float inv_norm, uint32_t
 }
 
 
+// Bitmap-mode key of an overlap accumulator (acc <= 64 * qpv < 2^24, so the
+// f32 conversion is exact).
+__device__ __forceinline__ uint32_t bm_key(const TcArgs& a, uint32_t acc) {
+  return a.key_kind == 0 ? a.n_top - acc : desc_key(__uint2float_rn(acc));
+}
+
+// Smallest accumulator whose key is <= thr; both key kinds are strictly
+// decreasing in acc, so key(acc) == thr exactly at acc == result when thr is
+// the key of some row.
+__device__ uint32_t bm_amin(const TcArgs& a, uint32_t thr) {
+  if (a.key_kind == 0) return thr >= a.n_top ? 0u : a.n_top - thr;
+  uint32_t lo = 0, hi = 64u * a.qpv + 1;
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if (bm_key(a, mid) <= thr)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  return lo;
+}
+
 __device__ __forceinline__ uint4 load_codes(const uint8_t* p) {
   uint4 v;
   asm volatile("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
@@ -178,8 +207,11 @@ __device__ __forceinline__ uint4 load_codes(const uint8_t* p) {
   return v;
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1)
-    fastscan_tc_kernel(const __grid_constant__ CUtensorMap lut_map, const TcArgs a) {
+// MODE 0: FastScan (A = one-hot of nibble codes, B = u8 LUTs, score by the
+// FastScan formula).  MODE 1: bitmap AND-overlap (A = doc bits as 0/1 bytes,
+// B = query bits as 0/1 bytes, acc = overlap, key = n_top - overlap).
+template <int MODE>
+__device__ __forceinline__ void tc_scan_body(const CUtensorMap& lut_map, const TcArgs& a) {
   extern __shared__ uint8_t smem_raw[];
   TcSmem& S = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -187,7 +219,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint32_t nt = a.nt;
   const uint32_t nqt = (uint32_t)((a.nq - q0) < nt ? (a.nq - q0) : nt);
   const uint64_t n_blocks = (a.n + 31) / 32;
-  const uint32_t n_kb = a.pairs_pad / 8;
+  const uint32_t n_kb = a.n_kb;
   const bool dense = a.keys != nullptr;
 
   if (warp == 0) {
@@ -211,11 +243,30 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
   for (uint32_t i = t; i < nt; i += kTcThreads) {
     const bool v = i < nqt;
-    S.bias[i] = v ? a.bias[q0 + i] : 0.0f;
-    S.invq[i] = v ? a.invq[q0 + i] : 0.0f;
+    S.bias[i] = (MODE == 0 && v) ? a.bias[q0 + i] : 0.0f;
+    S.invq[i] = (MODE == 0 && v) ? a.invq[q0 + i] : 0.0f;
     S.thr[i] = (v && !dense) ? a.thr[(q0 + i) * a.thr_stride] : 0u;
-    S.amin[i] = !v ? kNeverPasses
-                   : dense ? kExactCompare : filter_amin(S.bias[i], S.invq[i], a.inv_norm, S.thr[i], 255u * a.pairs_pad);
+    if (MODE == 0)
+      S.amin[i] = !v ? kNeverPasses
+                     : dense ? kExactCompare
+                             : filter_amin(S.bias[i], S.invq[i], a.inv_norm, S.thr[i], 255u * a.pairs_pad);
+    else if (!v || dense)
+      S.amin[i] = v ? 0u : kNeverPasses;
+    else {
+      // key <= thr  <=>  acc >= am.  With a tie bound, (key, doc) <= (thr, tdoc):
+      // this tile's docs [first, first + 256) all pass the tie level, none do,
+      // or the compare is per doc (kExactCompare, am kept in thr).
+      const uint32_t am = bm_amin(a, S.thr[i]);
+      S.amin[i] = am;
+      if (a.thr_pos) {
+        const uint32_t p = a.thr_pos[(q0 + i) * a.thr_stride];
+        const uint64_t td = ((uint64_t)(p >> 5) * a.smp_stride) * 32 + (p & 31);
+        const uint64_t first = (uint64_t)blockIdx.x * kTcM;
+        S.tdoc[i] = (uint32_t)td;
+        S.thr[i] = am;
+        S.amin[i] = td >= first + kTcM - 1 ? am : td < first ? am + 1 : kExactCompare;
+      }
+    }
     S.cnt[i] = 0;
   }
   __syncthreads();  // barrier init and amin visible to every thread
@@ -286,6 +337,56 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // ---- A builders: row r = doc (tile-local), chunks 4*hc .. 4*hc+3 ----------
     const uint32_t bt = (uint32_t)t - 64;
     const uint32_t r = bt & 255, hc = bt >> 8;
+    if constexpr (MODE == 1) {
+      // bitmap rows, bit j of word j/64 = coordinate j: thread hc expands word
+      // 2 kb + hc (coordinates 64 hc .. 64 hc + 63 of K-block kb) to 0/1 bytes
+      const uint64_t pb = ((uint64_t)blockIdx.x * 8 + (r >> 5)) * a.block_stride;
+      const uint64_t doc = pb * 32 + (r & 31);
+      const bool row_ok = pb < n_blocks && doc < a.n;
+      const uint64_t* words = reinterpret_cast<const uint64_t*>(a.blocks) + (row_ok ? doc : 0) * (uint64_t)a.qpv;
+      const uint32_t a_row = smem_u32(S.a[0]) + (r >> 7) * kAHalf + ((r & 127) >> 3) * 1024 + (r & 7) * 128;
+      uint32_t dst[4];
+#pragma unroll
+      for (uint32_t c = 0; c < 4; c++) dst[c] = a_row + (((4 * hc + c) ^ (r & 7)) << 4);
+      auto word_at = [&](uint32_t kb) -> uint64_t {
+        const uint32_t wi = 2 * kb + hc;
+        return (row_ok && wi < a.qpv) ? __ldg(words + wi) : 0ull;
+      };
+      uint32_t s = 0, par = 0, base = 0;
+      bool ok = true;
+      uint64_t nxt = word_at(0);
+      for (uint32_t kb = 0; kb < n_kb && ok; kb++) {
+        const uint64_t wd = nxt;
+        if (kb + 1 < n_kb) nxt = word_at(kb + 1);
+        if (kb >= (uint32_t)kTcStages) {
+          if (lane == 0) ok = mbar_wait(&S.empty[s], par ^ 1);
+          ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
+          if (!ok) {
+            if (lane == 0) raise_abort(S, a.err);
+            break;
+          }
+          __syncwarp();
+        }
+#pragma unroll
+        for (uint32_t c = 0; c < 4; c++) {  // 16 coordinates per 16-byte chunk
+          const uint32_t h = (uint32_t)(wd >> (16 * c));
+          uint32_t o[4];
+#pragma unroll
+          for (uint32_t i = 0; i < 4; i++)  // 4 bits -> 4 bytes (the shifted copies never overlap)
+            o[i] = (((h >> (4 * i)) & 15u) * 0x00204081u) & 0x01010101u;
+          st_shared_v4(dst[c] + base, o[0], o[1], o[2], o[3]);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&S.full_a[s]);
+        base += kAStage;
+        if (++s == kTcStages) {
+          s = 0;
+          base = 0;
+          par ^= 1;
+        }
+      }
+    } else
     {
       const uint64_t pb = ((uint64_t)blockIdx.x * 8 + (r >> 5)) * a.block_stride;
       const bool row_valid = pb < n_blocks;
@@ -392,7 +493,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           for (uint32_t j = 0; j < 32; j++) {
             const uint32_t q = cb + j;
             if (valid && q < nqt)
-              a.keys[(q0 + q) * a.ld + u] = desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm));
+              a.keys[(q0 + q) * a.ld + u] =
+                  MODE == 0 ? desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm)) : bm_key(a, v[j]);
           }
           continue;
         }
@@ -407,9 +509,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           for (uint32_t j = 0; j < 32; j++) {
             const uint32_t q = cb + j;  // < kTcMaxN; same q in every lane
             const uint32_t am = S.amin[q];
-            const bool pass = am != kExactCompare
-                                  ? v[j] >= am
-                                  : desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm)) <= S.thr[q];
+            bool pass;
+            if (am != kExactCompare)
+              pass = v[j] >= am;
+            else if (MODE == 0)
+              pass = desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm)) <= S.thr[q];
+            else
+              pass = v[j] > S.thr[q] || (v[j] == S.thr[q] && doc <= S.tdoc[q]);
             m[j] = __ballot_sync(0xFFFFFFFFu, valid & pass);
           }
         }
@@ -444,7 +550,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           const uint32_t q = en.y & 255, li = (en.y >> 8) & 255, rw = en.y >> 16;
           const uint32_t pos = S.base[q] + li;
           if (pos < a.cap) {
-            a.f_keys[(q0 + q) * a.cap + pos] = desc_key(tc_score(en.x, S.bias[q], S.invq[q], a.inv_norm));
+            a.f_keys[(q0 + q) * a.cap + pos] =
+                MODE == 0 ? desc_key(tc_score(en.x, S.bias[q], S.invq[q], a.inv_norm)) : bm_key(a, en.x);
             const uint64_t rpb = ((uint64_t)blockIdx.x * 8 + (rw >> 5)) * a.block_stride;
             a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw & 31));
           }
@@ -458,6 +565,28 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
+__global__ void __launch_bounds__(kTcThreads, 1)
+    fastscan_tc_kernel(const __grid_constant__ CUtensorMap lut_map, const TcArgs a) {
+  tc_scan_body<0>(lut_map, a);
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    bitmap_tc_kernel(const __grid_constant__ CUtensorMap q_map, const TcArgs a) {
+  tc_scan_body<1>(q_map, a);
+}
+
+// query bits (qpv u64 words per query) -> 0/1 bytes, row_bytes per query
+__global__ void expand_query_bits_kernel(const uint64_t* __restrict__ qbits, uint64_t nq, uint32_t qpv,
+                                         uint32_t row_bytes, uint8_t* __restrict__ out) {
+  const uint64_t total = nq * (uint64_t)row_bytes;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t q = t / row_bytes;
+    const uint32_t j = (uint32_t)(t % row_bytes);
+    out[t] = (j / 64 < qpv) ? (uint8_t)((qbits[q * qpv + j / 64] >> (j % 64)) & 1ull) : 0;
+  }
+}
+
 __global__ void filter_check_kernel(const uint32_t* __restrict__ cnt, uint64_t nq, uint32_t need, uint32_t cap,
                                     uint32_t* __restrict__ flag) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -468,9 +597,12 @@ __global__ void filter_check_kernel(const uint32_t* __restrict__ cnt, uint64_t n
 }
 
 
-void launch_tc(TcArgs a, const uint8_t* lut, cudaStream_t stream) {
+template <int MODE>
+void launch_tc(TcArgs a, const uint8_t* b_rows, cudaStream_t stream) {
   if (!a.n || !a.nq) return;
-  const uint64_t k_bytes = (uint64_t)a.pairs_pad * 16;
+  const char* what = MODE == 0 ? "FastScan tensor-core scan" : "bitmap tensor-core scan";
+  const uint64_t k_bytes = (uint64_t)a.n_kb * kTcKBytes;
+  if (!a.n_kb || (MODE == 0 && a.n_kb % 4)) throw std::invalid_argument(std::string(what) + ": bad K extent");
   // N per tile: a multiple of 16 in [16, 256]
   a.nt = a.nq >= kTcMaxN ? kTcMaxN : (uint32_t)((a.nq + 15) / 16 * 16);
   CUtensorMap map;
@@ -478,22 +610,26 @@ void launch_tc(TcArgs a, const uint8_t* lut, cudaStream_t stream) {
   cuuint64_t gstride[1] = {(cuuint64_t)k_bytes};
   cuuint32_t box[2] = {(cuuint32_t)kTcKBytes, (cuuint32_t)a.nt};
   cuuint32_t estride[2] = {1, 1};
-  CUresult rc = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)lut, gdim, gstride, box, estride,
+  CUresult rc = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)b_rows, gdim, gstride, box, estride,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (rc != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed for the FastScan LUT matrix");
-  if (255ull * a.pairs_pad >= (1ull << 23))  // acc_to_float range
-    throw std::invalid_argument("FastScan tensor-core scan: dimension too large");
+  if (rc != CUDA_SUCCESS) throw CudaError(std::string("cuTensorMapEncodeTiled failed: ") + what);
+  if (MODE == 0 && 255ull * a.pairs_pad >= (1ull << 23))  // acc_to_float range
+    throw std::invalid_argument(std::string(what) + ": dimension too large");
+  if (MODE == 1 && (64ull * a.qpv >= (1ull << 24) || 2ull * a.n_kb < a.qpv))
+    throw std::invalid_argument(std::string(what) + ": row too long");
+  if (!a.keys && a.block_stride != 1) throw std::invalid_argument(std::string(what) + ": filter needs stride 1");
+  auto kernel = MODE == 0 ? fastscan_tc_kernel : bitmap_tc_kernel;
   const size_t smem = sizeof(TcSmem) + 1024;
-  OVB_CUDA(cudaFuncSetAttribute(fastscan_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  OVB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const uint64_t n_blocks = (a.n + 31) / 32;
   const uint64_t logical_blocks = (n_blocks + a.block_stride - 1) / a.block_stride;
   const uint64_t doc_tiles = (logical_blocks + 7) / 8;
   const uint64_t q_tiles = (a.nq + a.nt - 1) / a.nt;
-  if (q_tiles > 65535 || doc_tiles > 0x7FFFFFFF)
-    throw std::invalid_argument("FastScan tensor-core scan: grid too large; split the query batch");
+  if (q_tiles > 65535 || doc_tiles > 0x7FFFFFFF || a.n >= (1ull << 32))
+    throw std::invalid_argument(std::string(what) + ": grid too large; split the query batch");
   dim3 grid((unsigned)doc_tiles, (unsigned)q_tiles);
-  fastscan_tc_kernel<<<grid, kTcThreads, smem, stream>>>(map, a);
+  kernel<<<grid, kTcThreads, smem, stream>>>(map, a);
   launched();
 }
 
@@ -515,6 +651,7 @@ void launch_fastscan_scan_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_p
   a.blocks = blocks;
   a.n = n;
   a.pairs_pad = pairs_pad;
+  a.n_kb = pairs_pad / 8;
   a.block_stride = block_stride ? block_stride : 1;
   a.bias = bias_sum;
   a.invq = inv_q;
@@ -523,7 +660,7 @@ void launch_fastscan_scan_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_p
   a.keys = keys;
   a.ld = ld;
   a.err = err;
-  launch_tc(a, lut, stream);
+  launch_tc<0>(a, lut, stream);
 }
 
 void launch_fastscan_filter_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad, const uint8_t* lut,
@@ -534,6 +671,7 @@ void launch_fastscan_filter_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs
   a.blocks = blocks;
   a.n = n;
   a.pairs_pad = pairs_pad;
+  a.n_kb = pairs_pad / 8;
   a.block_stride = 1;
   a.bias = bias_sum;
   a.invq = inv_q;
@@ -546,7 +684,61 @@ void launch_fastscan_filter_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs
   a.f_keys = f_keys;
   a.f_ids = f_ids;
   a.err = err;
-  launch_tc(a, lut, stream);
+  launch_tc<0>(a, lut, stream);
+}
+
+uint32_t bitmap_tc_kblocks(uint32_t qpv) { return (qpv + 1) / 2; }
+
+void launch_bitmap_tc_query(const uint64_t* qbits, uint64_t nq, uint32_t qpv, uint8_t* out, cudaStream_t stream) {
+  if (!nq) return;
+  const uint32_t row = bitmap_tc_kblocks(qpv) * kTcKBytes;
+  uint64_t blocks = (nq * row + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  expand_query_bits_kernel<<<(unsigned)blocks, 256, 0, stream>>>(qbits, nq, qpv, row, out);
+  launched();
+}
+
+void launch_bitmap_scan_tc(const uint64_t* words, uint64_t n, uint32_t qpv, uint32_t key_kind, uint32_t n_top,
+                           const uint8_t* q_bytes, uint64_t nq, uint32_t block_stride, uint32_t* keys, uint64_t ld,
+                           uint32_t* err, cudaStream_t stream) {
+  TcArgs a{};
+  a.blocks = reinterpret_cast<const uint8_t*>(words);
+  a.n = n;
+  a.qpv = qpv;
+  a.n_kb = bitmap_tc_kblocks(qpv);
+  a.key_kind = key_kind;
+  a.n_top = n_top;
+  a.block_stride = block_stride ? block_stride : 1;
+  a.nq = nq;
+  a.keys = keys;
+  a.ld = ld;
+  a.err = err;
+  launch_tc<1>(a, q_bytes, stream);
+}
+
+void launch_bitmap_filter_tc(const uint64_t* words, uint64_t n, uint32_t qpv, uint32_t key_kind, uint32_t n_top,
+                             const uint8_t* q_bytes, uint64_t nq, const uint32_t* thr, const uint32_t* thr_pos,
+                             uint32_t smp_stride, uint64_t thr_stride, uint32_t* cnt, uint32_t cap, uint32_t* f_keys,
+                             uint32_t* f_ids, uint32_t* err, cudaStream_t stream) {
+  TcArgs a{};
+  a.blocks = reinterpret_cast<const uint8_t*>(words);
+  a.n = n;
+  a.qpv = qpv;
+  a.n_kb = bitmap_tc_kblocks(qpv);
+  a.key_kind = key_kind;
+  a.n_top = n_top;
+  a.block_stride = 1;
+  a.nq = nq;
+  a.thr = thr;
+  a.thr_pos = thr_pos;
+  a.smp_stride = smp_stride ? smp_stride : 1;
+  a.thr_stride = thr_stride;
+  a.cnt = cnt;
+  a.cap = cap;
+  a.f_keys = f_keys;
+  a.f_ids = f_ids;
+  a.err = err;
+  launch_tc<1>(a, q_bytes, stream);
 }
 
 void launch_filter_check(const uint32_t* cnt, uint64_t nq, uint32_t need, uint32_t cap, uint32_t* flag,

@@ -567,6 +567,98 @@ def test_sign_score_all_and_top_m(orc, corpus):
         assert np.array_equal(got[qi], orc.sign_top_m(words, n, dim, queries[qi], 320))
 
 
+_BITMAP_ENV = ("OVB_BITMAP_TC", "OVB_FASTSCAN_FILTER", "OVB_FASTSCAN_SAMPLE_MULT")
+
+
+def _bitmap_modes(monkeypatch, fn, **env):
+    """fn() once per environment setting; returns the results in order."""
+    out = []
+    for settings in env.values():
+        for var in _BITMAP_ENV:
+            monkeypatch.delenv(var, raising=False)
+        for var, val in settings.items():
+            monkeypatch.setenv(var, val)
+        out.append(fn())
+    for var in _BITMAP_ENV:
+        monkeypatch.delenv(var, raising=False)
+    return out
+
+
+_BITMAP_THREE = dict(
+    filt={"OVB_BITMAP_TC": "1", "OVB_FASTSCAN_FILTER": "1"},
+    dense={"OVB_BITMAP_TC": "1", "OVB_FASTSCAN_FILTER": "0"},
+    cuda_core={"OVB_BITMAP_TC": "0"},
+)
+
+
+@pytest.mark.parametrize(
+    "dim,n_top,n,nq,m,mult",
+    [
+        (768, 192, 40_000, 70, 500, None),    # 6 K-blocks, sample stride 4
+        (320, 80, 39_950, 40, 300, None),     # odd word count (half K-block), partial last tile
+        (64, 16, 70_001, 300, 700, None),     # one word per row, two query tiles, massive key ties
+        (768, 192, 40_000, 70, 500, "0.02"),  # threshold too tight -> dense redo
+        (768, 192, 40_000, 70, 500, "1e6"),   # keeps everything -> over capacity -> dense redo
+    ],
+)
+def test_bitmap_tensor_core_top_m_is_exact(orc, monkeypatch, dim, n_top, n, nq, m, mult):
+    """Constant-weight bitmap candidates from the tensor-core overlap scan
+    (sample threshold with a (key, doc) tie bound, and the dense key matrix)
+    equal the CUDA-core popcount scan and the oracle, ids in tie order."""
+    docs = ob.synth_docs(43, n, dim)
+    queries, _ = ob.synth_queries(43, n, nq, dim)
+    bm = ob.Bitmap(dim, n_top)
+    bm.add(docs)
+    env = dict(_BITMAP_THREE)
+    if mult:
+        env["filt"] = dict(env["filt"], OVB_FASTSCAN_SAMPLE_MULT=mult)
+    f, d, c = _bitmap_modes(monkeypatch, lambda: bm.top_m_candidates_batched(queries, m), **env)
+    assert np.array_equal(f, d) and np.array_equal(f, c)
+    words = orc.bitmap_encode(docs, dim, n_top)
+    for qi in (0, nq // 2, nq - 1):
+        assert np.array_equal(f[qi], orc.bitmap_top_m(words, n, dim, n_top, queries[qi], m)), qi
+    fs, ds = _bitmap_modes(monkeypatch, lambda: bm.search(queries, 50), filt=env["filt"], cuda_core={"OVB_BITMAP_TC": "0"})
+    assert np.array_equal(fs.indices, ds.indices) and np.array_equal(fs.scores, ds.scores)
+
+
+def test_bitmap_tensor_core_duplicate_rows(orc, monkeypatch):
+    """400 distinct rows tiled 100x: every key level holds >= 100 docs, so the
+    tie bound alone decides which equal-key docs the filter keeps."""
+    dim, n_top, base, reps, nq, m = 256, 64, 400, 100, 48, 1000
+    docs = np.tile(ob.synth_docs(47, base, dim), (reps, 1))
+    n = len(docs)
+    queries, _ = ob.synth_queries(47, base, nq, dim)
+    bm = ob.Bitmap(dim, n_top)
+    bm.add(docs)
+    f, d, c = _bitmap_modes(monkeypatch, lambda: bm.top_m_candidates_batched(queries, m), **_BITMAP_THREE)
+    assert np.array_equal(f, d) and np.array_equal(f, c)
+    words = orc.bitmap_encode(docs, dim, n_top)
+    assert np.array_equal(f[5], orc.bitmap_top_m(words, n, dim, n_top, queries[5], m))
+
+
+def test_multibucket_identity_weights_tensor_core(orc, monkeypatch):
+    """Identity (diagonal) weights take the tensor-core overlap scan: same ids
+    as the weighted CUDA-core scan and the oracle; other weights do not change."""
+    n, dim, bits, nq, m = 45_000, 768, 2, 64, 600
+    docs = ob.synth_docs(53, n, dim)
+    queries, _ = ob.synth_queries(53, n, nq, dim)
+    mb = ob.MultiBucketBitmap(dim, bits)
+    mb.add(docs)
+    w = orc.multibucket_weights(bits, "diagonal")
+    f, d, c = _bitmap_modes(monkeypatch, lambda: mb.top_m_bilinear_batched(queries, w, m), **_BITMAP_THREE)
+    assert np.array_equal(f, d) and np.array_equal(f, c)
+    words = orc.multibucket_encode(docs, dim, bits)
+    for qi in (0, 33):
+        qbm = orc.multibucket_query(queries[qi], dim, bits)
+        assert np.array_equal(f[qi], orc.multibucket_top_m(words, n, dim, bits, qbm, w, m)), qi
+    wo = orc.multibucket_weights(bits, "outer")
+    a, b = _bitmap_modes(monkeypatch, lambda: mb.top_m_bilinear_batched(queries[:40], wo, m),
+                         tc={"OVB_BITMAP_TC": "1"}, cuda_core={"OVB_BITMAP_TC": "0"})
+    assert np.array_equal(a, b)
+    qbm = orc.multibucket_query(queries[1], dim, bits)
+    assert np.array_equal(a[1], orc.multibucket_top_m(words, n, dim, bits, qbm, wo, m))
+
+
 # ------------------------------------------------------------ multi-bucket
 @pytest.mark.parametrize("kind", ["diagonal", "outer", "banded"])
 def test_multibucket_top_m_exact(orc, kind):
