@@ -354,10 +354,15 @@ __device__ __forceinline__ void tc_scan_body(const CUtensorMap& lut_map, const T
       };
       uint32_t s = 0, par = 0, base = 0;
       bool ok = true;
-      uint64_t nxt = word_at(0);
+      // four K-blocks of words in flight (the tile's first loads are the
+      // latency that is not hidden)
+      uint64_t w0 = word_at(0), w1 = word_at(1), w2 = word_at(2), w3 = word_at(3);
       for (uint32_t kb = 0; kb < n_kb && ok; kb++) {
-        const uint64_t wd = nxt;
-        if (kb + 1 < n_kb) nxt = word_at(kb + 1);
+        const uint64_t wd = w0;
+        w0 = w1;
+        w1 = w2;
+        w2 = w3;
+        w3 = kb + 4 < n_kb ? word_at(kb + 4) : 0ull;
         if (kb >= (uint32_t)kTcStages) {
           if (lane == 0) ok = mbar_wait(&S.empty[s], par ^ 1);
           ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
@@ -498,12 +503,17 @@ __device__ __forceinline__ void tc_scan_body(const CUtensorMap& lut_map, const T
           }
           continue;
         }
-        // filter: 32 independent compares + ballots (amin is kNeverPasses past
-        // nqt), then the appends at prefix offsets of the ballots; no atomics
-        uint32_t m[32];
+        // filter: each lane (row) builds the mask of the 32 queries its doc
+        // passes (amin is kNeverPasses past nqt); kept docs are rare (m << n),
+        // so the appends run once per set bit of the busiest lane's mask
+        uint32_t hm = 0;
         if (!any_exact) {  // the common case: accumulator compares only
 #pragma unroll
-          for (uint32_t j = 0; j < 32; j++) m[j] = __ballot_sync(0xFFFFFFFFu, valid & (v[j] >= S.amin[cb + j]));
+          for (uint32_t j = 0; j < 32; j += 4) {
+            const uint4 am = *reinterpret_cast<const uint4*>(&S.amin[cb + j]);
+            hm |= ((uint32_t)(v[j] >= am.x) << j) | ((uint32_t)(v[j + 1] >= am.y) << (j + 1)) |
+                  ((uint32_t)(v[j + 2] >= am.z) << (j + 2)) | ((uint32_t)(v[j + 3] >= am.w) << (j + 3));
+          }
         } else {
 #pragma unroll
           for (uint32_t j = 0; j < 32; j++) {
@@ -516,14 +526,24 @@ __device__ __forceinline__ void tc_scan_body(const CUtensorMap& lut_map, const T
               pass = desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm)) <= S.thr[q];
             else
               pass = v[j] > S.thr[q] || (v[j] == S.thr[q] && doc <= S.tdoc[q]);
-            m[j] = __ballot_sync(0xFFFFFFFFu, valid & pass);
+            hm |= (uint32_t)pass << j;
           }
         }
+        if (!valid) hm = 0;
+        // appends at ballot-prefix offsets of the warp's segment; no atomics
+        while (__any_sync(0xFFFFFFFFu, hm != 0)) {
+          const bool has = hm != 0;
+          const uint32_t j = has ? (uint32_t)(__ffs(hm) - 1) : 0u;
+          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+          const uint32_t e = wcount + __popc(bal & lt);
+          if (has && e < kSegCap) {
+            uint32_t acc = v[0];
 #pragma unroll
-        for (uint32_t j = 0; j < 32; j++) {
-          const uint32_t e = wcount + __popc(m[j] & lt);
-          if (((m[j] >> lane) & 1) && e < kSegCap) list[e] = make_uint2(v[j], (cb + j) | (row << 16));
-          wcount += __popc(m[j]);
+            for (uint32_t jj = 1; jj < 32; jj++) acc = jj == j ? v[jj] : acc;
+            list[e] = make_uint2(acc, (cb + j) | (row << 16));
+          }
+          wcount += __popc(bal);
+          hm &= hm - 1;
         }
       }
       if (!dense) {
