@@ -190,7 +190,7 @@ uint32_t bitmap_subset(const Index& bm, const float* d_q, uint64_t nq, const uin
                      w.stream);
   SelectArgs a{keys, d_cands, d_off, 0, 0, ke, bits_for(bm.n_top), bits_for(bm.n ? bm.n - 1 : 0),
                (uint32_t*)w.out_keys.ensure(nq * ke * 4), (uint32_t*)w.out_ids.ensure(nq * ke * 4)};
-  size_t se = select_rows_scratch_elems(nq, ke);
+  size_t se = select_rows_scratch_elems(nq, ke, 0);
   launch_select_rows(a, nq, se ? (uint64_t*)w.scratch.ensure(se * 8) : nullptr, w.stream);
   return ke;
 }

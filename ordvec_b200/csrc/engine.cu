@@ -36,7 +36,7 @@ void select_rows(Workspace& w, const uint32_t* keys, const uint32_t* ids, const 
                  uint32_t id_bits, uint32_t* out_keys, uint32_t* out_ids, cudaStream_t st,
                  const uint32_t* row_len = nullptr) {
   SelectArgs a{keys, ids, row_off, ld, n, k, key_bits, id_bits, out_keys, out_ids, row_len};
-  size_t se = select_rows_scratch_elems(rows, k);
+  size_t se = select_rows_scratch_elems(rows, k, row_off ? 0 : n);
   uint64_t* scratch = se ? (uint64_t*)w.scratch.ensure(se * 8) : nullptr;
   launch_select_rows(a, rows, scratch, st);
 }

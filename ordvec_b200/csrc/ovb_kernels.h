@@ -24,7 +24,10 @@ struct SelectArgs {
   uint32_t* out_ids;
   const uint32_t* row_len;  // optional: row r holds min(row_len[r], n) entries at r*ld
 };
-size_t select_rows_scratch_elems(uint64_t rows, uint32_t k);
+// u64 scratch elements launch_select_rows may use for `rows` rows of length n
+// (0 for ragged rows): global sort buffers for k > kSelectSmemCap, and the
+// whole-GPU form's histograms and winners for a few rows of >= 2^20 keys.
+size_t select_rows_scratch_elems(uint64_t rows, uint32_t k, uint64_t n);
 void launch_select_rows(const SelectArgs& a, uint64_t rows, uint64_t* scratch,
                         cudaStream_t stream);
 

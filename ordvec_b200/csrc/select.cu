@@ -336,18 +336,251 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kSelThrea
   }
 }
 
+// Whole-GPU form for a few very long rows (one query per call over millions
+// of docs): each digit pass is one launch whose CTAs histogram grid-stride
+// slices of every row into a global histogram; the last CTA of a row to
+// finish (atomic arrival count after a fence) scans it, fixes the digit and
+// resets the histogram.  A collect launch gathers the winners the same way and
+// its last CTA per row sorts and writes them.  No CTA waits for another.
+constexpr uint32_t kWideRows = 16;
+constexpr uint64_t kWideMinN = 1u << 20;
+constexpr int kWideThreads = 512;
+
+struct WideState {
+  uint64_t prefix, fixed;
+  uint32_t need, done, arrive, below, tie, pad;
+};
+static_assert(sizeof(WideState) == 40, "WideState layout");
+
+struct WideScratch {
+  uint32_t* hist;    // rows x kHistBins
+  WideState* state;  // rows
+  uint64_t* win;     // rows x k
+};
+
+__host__ __device__ inline uint64_t wide_state_elems(uint64_t rows) { return (rows * sizeof(WideState) + 7) / 8; }
+
+__host__ inline WideScratch wide_scratch(uint64_t* scratch, uint64_t rows) {
+  WideScratch w;
+  w.hist = reinterpret_cast<uint32_t*>(scratch);
+  w.state = reinterpret_cast<WideState*>(scratch + rows * (kHistBins / 2));
+  w.win = scratch + rows * (kHistBins / 2) + wide_state_elems(rows);
+  return w;
+}
+
+__global__ void wide_init_kernel(SelectArgs a, WideScratch w) {
+  const uint64_t row = blockIdx.x;
+  for (uint32_t b = threadIdx.x; b < kHistBins; b += blockDim.x) w.hist[row * kHistBins + b] = 0;
+  if (threadIdx.x == 0) {
+    WideState& st = w.state[row];
+    st.prefix = 0;
+    st.fixed = 0;
+    st.need = (uint32_t)(a.n < a.k ? a.n : a.k);
+    st.done = st.need == a.n;  // every key is a winner
+    st.arrive = st.below = st.tie = st.pad = 0;
+  }
+}
+
+// Exclusive scan of hist[0..kHistBins) by kWideThreads threads (4 bins each);
+// the thread whose bins hold the need-th key writes (bin, before, in_bin).
+__device__ void wide_find_bin(const uint32_t* hist, uint32_t need, uint32_t* out3) {
+  __shared__ uint32_t warp_tot[kWideThreads / 32];
+  const uint32_t t = threadIdx.x, lane = t & 31, wp = t >> 5;
+  uint32_t h[4], sum = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    h[j] = hist[4 * t + j];
+    sum += h[j];
+  }
+  uint32_t incl = sum;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_tot[wp] = incl;
+  __syncthreads();
+  if (wp == 0) {
+    const uint32_t v = lane < kWideThreads / 32 ? warp_tot[lane] : 0;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane < kWideThreads / 32) warp_tot[lane] = x - v;
+  }
+  __syncthreads();
+  uint32_t before = warp_tot[wp] + incl - sum;
+  if (before < need && need <= before + sum) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if (need <= before + h[j]) {
+        out3[0] = 4 * t + j;
+        out3[1] = before;
+        out3[2] = h[j];
+        break;
+      }
+      before += h[j];
+    }
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kWideThreads) wide_hist_kernel(SelectArgs a, WideScratch w, uint32_t shift,
+                                                                 uint32_t width) {
+  __shared__ uint32_t hist[kHistBins];
+  __shared__ uint32_t s_last, s_pick[3];
+  const uint64_t row = blockIdx.y;
+  WideState& st = w.state[row];
+  if (*reinterpret_cast<volatile uint32_t*>(&st.done)) return;  // uniform per row
+  const uint64_t prefix = st.prefix, fixed = st.fixed;
+  const uint32_t mask = (1u << width) - 1;
+  for (uint32_t b = threadIdx.x; b < kHistBins; b += blockDim.x) hist[b] = 0;
+  __syncthreads();
+  const uint32_t* keys = a.keys + row * a.ld;
+  const uint32_t* ids = a.ids ? a.ids + row * a.ld : nullptr;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t key = load_key(keys, ids, i);
+    if ((key & fixed) == prefix) atomicAdd(&hist[(uint32_t)(key >> shift) & mask], 1u);
+  }
+  __syncthreads();
+  uint32_t* gh = w.hist + row * kHistBins;
+  for (uint32_t b = threadIdx.x; b <= mask; b += blockDim.x)
+    if (hist[b]) atomicAdd(&gh[b], hist[b]);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&st.arrive, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  // last CTA of this row: every other CTA's histogram is in gh
+  __threadfence();
+  for (uint32_t b = threadIdx.x; b < kHistBins; b += blockDim.x) {
+    hist[b] = b <= mask ? *reinterpret_cast<volatile uint32_t*>(&gh[b]) : 0u;
+    gh[b] = 0;
+  }
+  __syncthreads();
+  const uint32_t need = st.need;
+  wide_find_bin(hist, need, s_pick);
+  if (threadIdx.x == 0) {
+    st.need = need - s_pick[1];
+    st.prefix = prefix | ((uint64_t)s_pick[0] << shift);
+    st.fixed = fixed | ((uint64_t)mask << shift);
+    st.done = s_pick[2] == need - s_pick[1];  // the whole bin is taken
+    st.arrive = 0;
+  }
+}
+
+// Collect: keys strictly below the prefix, then `need` keys inside it; the last
+// CTA of a row sorts the k winners and writes them.
+__global__ void __launch_bounds__(kWideThreads) wide_collect_kernel(SelectArgs a, WideScratch w) {
+  __shared__ uint64_t buf[kSelectSmemCap];
+  __shared__ uint32_t s_last;
+  const uint64_t row = blockIdx.y;
+  WideState& st = w.state[row];
+  const uint64_t prefix = st.prefix, fixed = st.fixed;
+  const uint32_t k_eff = (uint32_t)(a.n < a.k ? a.n : a.k), need = st.need;
+  const uint32_t below_total = k_eff - need;
+  const uint32_t* keys = a.keys + row * a.ld;
+  const uint32_t* ids = a.ids ? a.ids + row * a.ld : nullptr;
+  uint64_t* win = w.win + row * (uint64_t)a.k;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  // warp-uniform trip count so the ballots see every lane
+  const uint64_t first = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+  for (uint64_t base = first; base < a.n; base += stride) {
+    const uint64_t i = base + lane;
+    uint64_t key = 0;
+    bool lo = false, eq = false;
+    if (i < a.n) {
+      key = load_key(keys, ids, i);
+      const uint64_t m = key & fixed;
+      lo = m < prefix;
+      eq = m == prefix;
+    }
+    uint32_t lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    const uint32_t bl = __ballot_sync(0xFFFFFFFFu, lo), be = __ballot_sync(0xFFFFFFFFu, eq);
+    uint32_t b0 = 0, e0 = 0;
+    if (lane == 0) {
+      if (bl) b0 = atomicAdd(&st.below, (uint32_t)__popc(bl));
+      if (be) e0 = atomicAdd(&st.tie, (uint32_t)__popc(be));
+    }
+    b0 = __shfl_sync(0xFFFFFFFFu, b0, 0);
+    e0 = __shfl_sync(0xFFFFFFFFu, e0, 0);
+    if (lo) {
+      const uint32_t slot = b0 + __popc(bl & lt);
+      if (slot < below_total) win[slot] = key;
+    } else if (eq) {
+      const uint32_t slot = e0 + __popc(be & lt);
+      if (slot < need) win[below_total + slot] = key;
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&st.arrive, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  uint32_t len = 1;
+  while (len < k_eff) len <<= 1;
+  for (uint32_t j = threadIdx.x; j < len; j += blockDim.x)
+    buf[j] = j < k_eff ? *reinterpret_cast<volatile uint64_t*>(&win[j]) : ~0ull;
+  __syncthreads();
+  bitonic_sort(buf, len);
+  uint32_t* out_k = a.out_keys + row * (uint64_t)a.k;
+  uint32_t* out_i = a.out_ids + row * (uint64_t)a.k;
+  for (uint32_t j = threadIdx.x; j < a.k; j += blockDim.x) {
+    out_k[j] = j < k_eff ? (uint32_t)(buf[j] >> 32) : kSentinelKey;
+    out_i[j] = j < k_eff ? (uint32_t)buf[j] : kSentinelId;
+  }
+}
+
+void launch_select_wide(const SelectArgs& a, uint64_t rows, uint64_t* scratch, cudaStream_t stream) {
+  const WideScratch w = wide_scratch(scratch, rows);
+  wide_init_kernel<<<(unsigned)rows, 256, 0, stream>>>(a, w);
+  uint64_t per_row = (a.n + kWideThreads * 32 - 1) / (kWideThreads * 32);  // ~32 keys per thread
+  const uint64_t cap = (148ull * 4 + rows - 1) / rows;
+  if (per_row > cap) per_row = cap;
+  if (per_row < 1) per_row = 1;
+  const dim3 grid((unsigned)per_row, (unsigned)rows);
+  for (int part = 0; part < 2; part++) {  // key bits, then id bits, 11 at a time from the top
+    uint32_t bits = part == 0 ? a.key_bits : a.id_bits;
+    uint32_t top = (part == 0 ? 32u : 0u) + bits;
+    while (bits > 0) {
+      const uint32_t wd = bits < 11 ? bits : 11;
+      top -= wd;
+      wide_hist_kernel<<<grid, kWideThreads, 0, stream>>>(a, w, top, wd);
+      bits -= wd;
+    }
+  }
+  wide_collect_kernel<<<grid, kWideThreads, 0, stream>>>(a, w);
+  launched();
+}
+
+bool use_select_wide(const SelectArgs& a, uint64_t rows, const uint64_t* scratch) {
+  return scratch && !a.row_off && !a.row_len && rows <= kWideRows && a.n >= kWideMinN && a.k <= kSelectSmemCap;
+}
+
 }  // namespace
 
-size_t select_rows_scratch_elems(uint64_t rows, uint32_t k) {
-  if (k <= kSelectSmemCap) return 0;
+size_t select_rows_scratch_elems(uint64_t rows, uint32_t k, uint64_t n) {
   uint64_t len = 1;
   while (len < k) len <<= 1;
-  return rows * len;
+  uint64_t e = k <= kSelectSmemCap ? 0 : rows * len;
+  if (rows <= kWideRows && k <= kSelectSmemCap && n >= kWideMinN) {  // the whole-GPU form for few long rows
+    const uint64_t wide = rows * (kHistBins / 2) + wide_state_elems(rows) + rows * (uint64_t)k;
+    if (wide > e) e = wide;
+  }
+  return e;
 }
 
 void launch_select_rows(const SelectArgs& a, uint64_t rows, uint64_t* scratch,
                         cudaStream_t stream) {
   if (rows == 0) return;
+  const char* wide_env = getenv("OVB_SELECT_WIDE");  // "0" keeps the cluster / per-row forms
+  if (!(wide_env && wide_env[0] == '0') && use_select_wide(a, rows, scratch)) {
+    launch_select_wide(a, rows, scratch, stream);
+    return;
+  }
   // few long rows: one 8-CTA cluster per row
   if (!a.row_off && !a.row_len && a.k <= kClusterCap && a.n >= 32768 && rows * kClusterCtas <= 2 * 148) {
     select_rows_cluster_kernel<<<(unsigned)(rows * kClusterCtas), kSelThreads, 0, stream>>>(a);

@@ -659,6 +659,41 @@ def test_multibucket_identity_weights_tensor_core(orc, monkeypatch):
     assert np.array_equal(a[1], orc.multibucket_top_m(words, n, dim, bits, qbm, wo, m))
 
 
+@pytest.mark.parametrize("nq", [1, 3, 16])
+def test_wide_select_few_long_rows(orc, monkeypatch, nq):
+    """Whole-GPU select for a few rows of >= 2^20 keys (one query per call over
+    a large index): heavy key ties, so the id digits decide; equal to the
+    cluster / per-row select and to the oracle."""
+    n, dim, n_top, m = 1_200_000, 64, 16, 3000
+    docs = ob.synth_docs(61, n, dim)
+    queries, _ = ob.synth_queries(61, n, nq, dim)
+    bm = ob.Bitmap(dim, n_top)
+    bm.add(docs)
+    wide = np.array(bm.top_m_candidates_batched(queries, m))
+    monkeypatch.setenv("OVB_SELECT_WIDE", "0")
+    other = np.array(bm.top_m_candidates_batched(queries, m))
+    monkeypatch.delenv("OVB_SELECT_WIDE")
+    assert np.array_equal(wide, other)
+    words = orc.bitmap_encode(docs, dim, n_top)
+    for qi in {0, nq - 1}:
+        assert np.array_equal(wide[qi], orc.bitmap_top_m(words, n, dim, n_top, queries[qi], m)), qi
+
+
+def test_wide_select_float_keys(monkeypatch):
+    """RankQuant plain search over 1.05M docs (32-bit float keys)."""
+    n, dim = 1_050_000, 256
+    docs = ob.synth_docs(67, n, dim)
+    queries, _ = ob.synth_queries(67, n, 2, dim)
+    rq = ob.RankQuant(dim, 2)
+    rq.add(docs)
+    a = rq.search_asymmetric(queries, 100)
+    monkeypatch.setenv("OVB_SELECT_WIDE", "0")
+    b = rq.search_asymmetric(queries, 100)
+    monkeypatch.delenv("OVB_SELECT_WIDE")
+    assert np.array_equal(a.indices, b.indices)
+    assert np.array_equal(a.scores.view(np.uint32), b.scores.view(np.uint32))
+
+
 # ------------------------------------------------------------ multi-bucket
 @pytest.mark.parametrize("kind", ["diagonal", "outer", "banded"])
 def test_multibucket_top_m_exact(orc, kind):
