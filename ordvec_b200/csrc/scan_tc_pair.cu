@@ -1,0 +1,604 @@
+// K3-TC / K2-TC on CTA pairs: the FastScan and bitmap tensor-core scans as a
+// persistent kernel whose clusters of two CTAs issue tcgen05.mma.cta_group::2.
+//
+// Why pairs.  One M=256 MMA spans the two SMs of a pair: each SM holds 128 doc
+// rows of A and half of the queries' B, and receives its 128 rows x N of the
+// accumulator.  Per SM and per MMA that halves the B bytes read from shared
+// memory (at M=128 x N=256 one SM's MMA reads 96 of the 128 bytes per clock
+// shared memory delivers, and the A builders need the rest), and it halves the
+// accumulator to 256 TMEM columns, so each SM holds two: the epilogue of one
+// tile overlaps the next tile's mainloop.  Persistence removes the per-CTA
+// setup (TMEM allocation, barrier init, the first loads' latency).
+//
+// Tiles: 256 docs (rank r of the pair: docs [256 d + 128 r, +128)) x nt <= 256
+// queries; tile t = cluster + i * clusters, doc tile t / q_tiles, query tile
+// t % q_tiles (query tiles inner: a doc tile's codes are reused from L2).
+//
+// Warp roles (704 threads per CTA):
+//   warp 0, lane 0   TMA producer: this CTA's nt/2 B rows of K-block kb ->
+//                    stage s (waits its own empty[s]; complete_tx on the
+//                    leader's full_b[s], whose expect_tx the leader posts for
+//                    both halves)
+//   warp 1           TMEM allocation for the pair (both CTAs); on the leader,
+//                    lane 0 issues the MMAs: waits the leader's full_a[s] /
+//                    full_b[s], 4 MMAs per K-block, commits to both CTAs'
+//                    empty[s]; after a tile's last K-block commits to both
+//                    CTAs' acc_full[b]; before a tile waits acc_empty[b]
+//   warps 2..5       A builders (both CTAs): a thread per doc row, 8 chunks
+//                    per K-block, one arrive per warp on the leader's full_a[s]
+//   warps 6..21      epilogue (both CTAs): TMEM lane quarter warp % 4, column
+//                    quarter (warp - 6) / 4; after reading the accumulator one
+//                    arrive per warp on the leader's acc_empty[b]
+// Every wait is bounded; a timeout sets bit 0 of *err and the abort flag of
+// both CTAs, every role stops issuing work, and both CTAs meet at the final
+// cluster barrier before freeing the tensor memory.
+//
+// Results are the one-CTA kernel's (scan_fastscan_tc.cu), bit for bit: same
+// integer accumulators, same key functions and filter rules.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "ovb_common.cuh"
+#include "ovb_kernels.h"
+#include "tc_common.cuh"
+#include "tc_scan.cuh"
+
+namespace ovb {
+
+namespace {
+
+using namespace tc;
+using namespace tcs;
+
+constexpr int kPBuildWarps = 4;  // warps 2..5: one thread per doc row
+constexpr int kPEpiWarps = 16;   // warps 6..21: four per TMEM lane quarter
+constexpr int kPThreads = 32 * (2 + kPBuildWarps + kPEpiWarps);
+constexpr int kPEpiThreads = kPEpiWarps * 32;
+constexpr int kPStages = 4;
+constexpr uint32_t kPRows = 128;  // docs per CTA per tile
+constexpr uint32_t kPMaxN = 256;
+constexpr uint32_t kPKBytes = 128;
+constexpr uint32_t kPAStage = kPRows * kPKBytes;        // 16 KiB
+constexpr uint32_t kPBStage = (kPMaxN / 2) * kPKBytes;  // 16 KiB: this CTA's half of B
+constexpr uint32_t kPSegCap = 256;                      // kept entries per epilogue warp per tile
+constexpr uint32_t kPTmemCols = 512;                    // two accumulators of 256 columns
+
+struct PSmem {
+  uint8_t a[kPStages][kPAStage];
+  uint8_t b[kPStages][kPBStage];
+  uint2 list[kPEpiWarps][kPSegCap];  // (accumulator, q | slot << 8 | row << 16)
+  float bias[kPMaxN];
+  float invq[kPMaxN];
+  uint32_t thr[kPMaxN];
+  uint32_t amin[kPMaxN];
+  uint32_t tdoc[kPMaxN];
+  uint32_t cnt[kPMaxN];
+  uint32_t base[kPMaxN];
+  uint64_t full_a[kPStages];
+  uint64_t full_b[kPStages];
+  uint64_t empty[kPStages];
+  uint64_t acc_full[2];
+  uint64_t acc_empty[2];
+  uint32_t tmem;
+  uint32_t abort;
+  uint32_t epi_stop;   // epilogue: stop after this tile (written before an epilogue barrier)
+  uint32_t seg_full;   // filter: some warp's list segment overflowed in this tile
+  uint32_t any_exact;  // filter: some query of this tile needs key compares
+};
+
+__device__ __forceinline__ uint32_t cta_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+// shared::cluster address of the same object in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t peer_addr(uint32_t local, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// Arrive on a barrier at a cluster address (either CTA of the pair), with the
+// instruction's default (release, CTA-scope) semantics: a release at cluster
+// scope costs each arriving warp about half a microsecond.
+__device__ __forceinline__ void arrive_remote(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+
+// Barriers with arrivals from the other CTA are waited like local ones.
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity) { return mbar_wait(bar, parity); }
+
+__device__ __forceinline__ bool aborted(const PSmem& S) {
+  return *reinterpret_cast<const volatile uint32_t*>(&S.abort) != 0;
+}
+
+// Sets the abort flag of both CTAs and bit 0 of *err.
+__device__ __forceinline__ void raise_abort(PSmem& S, uint32_t* err) {
+  atomicExch(&S.abort, 1u);
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(peer_addr(smem_u32(&S.abort), cta_rank() ^ 1)), "r"(1u)
+               : "memory");
+  atomicOr(err, 1u);
+}
+
+// TMA tile load of this CTA's B rows; the transaction bytes land on the
+// barrier at cluster address `bar` (the leader's).
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+      "%4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_i8_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// Arrive-one on the barrier at cluster address `bar` when every MMA this
+// thread issued so far has completed.
+__device__ __forceinline__ void commit_pair(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// named barrier 1 over the epilogue warps
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kPEpiThreads) : "memory"); }
+
+struct PairGrid {
+  uint32_t n_doc_tiles, q_tiles;
+};
+
+template <int MODE>
+__device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs& a, const PairGrid g) {
+  extern __shared__ uint8_t smem_raw[];
+  PSmem& S = *reinterpret_cast<PSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const uint32_t rank = cta_rank();
+  const uint32_t cluster = blockIdx.x >> 1, n_clusters = gridDim.x >> 1;
+  const uint64_t total = (uint64_t)g.n_doc_tiles * g.q_tiles;
+  const uint32_t nt = a.nt, half = nt / 2;
+  const uint32_t n_kb = a.n_kb;
+  const uint64_t n_blocks = (a.n + 31) / 32;
+  const bool dense = a.keys != nullptr;
+
+  if (t == 32) {
+    for (int s = 0; s < kPStages; s++) {
+      mbar_init(&S.full_a[s], 2 * kPBuildWarps);  // builder warps of both CTAs
+      mbar_init(&S.full_b[s], 1);                 // the leader's expect_tx
+      mbar_init(&S.empty[s], 1);                  // the leader's MMA commit
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&S.acc_full[b], 1);
+      mbar_init(&S.acc_empty[b], 2 * kPEpiWarps);  // epilogue warps of both CTAs
+    }
+    S.abort = 0;
+    S.epi_stop = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
+                 "r"(kPTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  cluster_sync_all();  // both CTAs' barriers initialised, TMEM allocated
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = S.tmem;
+
+  if (warp == 0) {
+    // ---- TMA producer (both CTAs) ----------------------------------------------
+    if (lane == 0) {
+      uint64_t it = 0;  // K-blocks issued
+      for (uint64_t tile = cluster; tile < total && !aborted(S); tile += n_clusters) {
+        const uint64_t q0 = (tile % g.q_tiles) * nt;
+        for (uint32_t kb = 0; kb < n_kb; kb++, it++) {
+          const uint32_t s = (uint32_t)(it % kPStages);
+          if (aborted(S)) break;
+          if (it >= (uint64_t)kPStages && !mbar_wait(&S.empty[s], (uint32_t)((it / kPStages - 1) & 1))) {
+            raise_abort(S, a.err);
+            break;
+          }
+          if (rank == 0) mbar_expect_tx(&S.full_b[s], nt * kPKBytes);  // both halves
+          tma_load_2d_pair(S.b[s], &b_map, (int)(kb * kPKBytes), (int)(q0 + rank * half),
+                           peer_addr(smem_u32(&S.full_b[s]), 0));
+        }
+      }
+      // the leader waits (bounded) until its last copies, and the peer's, landed
+      if (rank == 0)
+        for (uint64_t j = it > (uint64_t)kPStages ? it - kPStages : 0; j < it; j++)
+          mbar_wait_cluster(&S.full_b[j % kPStages], (uint32_t)((j / kPStages) & 1));
+    }
+  } else if (warp == 1) {
+    // ---- MMA issuer (leader) ------------------------------------------------------
+    if (lane == 0 && rank == 0) {
+      // D s32, A/B u8, K-major, N = nt, M = 256 across the pair
+      const uint32_t idesc = (2u << 4) | ((nt >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
+      uint64_t it = 0, issued = 0;
+      uint32_t tcount = 0;
+      bool ok = true;
+      for (uint64_t tile = cluster; tile < total && ok; tile += n_clusters, tcount++) {
+        const uint32_t b = tcount & 1;
+        if (tcount >= 2 && !mbar_wait_cluster(&S.acc_empty[b], ((tcount >> 1) - 1) & 1)) ok = false;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t d = tmem + b * 256;
+        for (uint32_t kb = 0; kb < n_kb && ok; kb++, it++) {
+          const uint32_t s = (uint32_t)(it % kPStages), par = (uint32_t)((it / kPStages) & 1);
+          if (aborted(S) || !mbar_wait_cluster(&S.full_b[s], par) || !mbar_wait_cluster(&S.full_a[s], par)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a0 = smem_u32(S.a[s]), b0 = smem_u32(S.b[s]);
+#pragma unroll
+          for (uint32_t j = 0; j < 4; j++)
+            mma_i8_pair(d, sw128_desc(a0 + 32 * j), sw128_desc(b0 + 32 * j), idesc, (kb | j) != 0);
+          commit_pair(smem_u32(&S.empty[s]));
+          commit_pair(peer_addr(smem_u32(&S.empty[s]), 1));
+          issued = it + 1;
+        }
+        if (!ok) break;
+        commit_pair(smem_u32(&S.acc_full[b]));
+        commit_pair(peer_addr(smem_u32(&S.acc_full[b]), 1));
+      }
+      if (!ok) {
+        if (!aborted(S)) raise_abort(S, a.err);
+        // no MMA in flight when the pair frees its tensor memory
+        if (issued > 0)
+          mbar_wait(&S.empty[(issued - 1) % kPStages], (uint32_t)(((issued - 1) / kPStages) & 1));
+      }
+    }
+  } else if (warp < 2 + kPBuildWarps) {
+    // ---- A builders (both CTAs): thread r builds doc row r, chunks 0..7 ---------------
+    const uint32_t r = (uint32_t)t - 64;  // 0..127
+    const uint32_t a_row = (r >> 3) * 1024 + (r & 7) * 128;
+    const uint32_t full_a0 = peer_addr(smem_u32(&S.full_a[0]), 0);  // leader's full_a[0]
+    uint64_t it = 0;
+    bool ok = true;
+    // wait for stage s to be free, or stop (warp-uniform)
+    auto acquire = [&](uint32_t s) -> bool {
+      bool w = true;
+      if (it >= (uint64_t)kPStages) {
+        if (lane == 0) w = !aborted(S) && mbar_wait(&S.empty[s], (uint32_t)((it / kPStages - 1) & 1));
+        w = __shfl_sync(0xFFFFFFFFu, w, 0);
+        if (!w && lane == 0 && !aborted(S)) raise_abort(S, a.err);
+        __syncwarp();
+      }
+      return w;
+    };
+    auto publish = [&](uint32_t s) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) arrive_remote(full_a0 + 8 * s);
+    };
+    for (uint64_t tile = cluster; tile < total && ok; tile += n_clusters) {
+      const uint64_t dt = tile / g.q_tiles;
+      const uint64_t pb = (dt * 8 + rank * 4 + (r >> 5)) * a.block_stride;
+      const uint64_t doc = pb * 32 + (r & 31);
+      if constexpr (MODE == 1) {
+        const bool row_ok = pb < n_blocks && doc < a.n;
+        const uint64_t* words = reinterpret_cast<const uint64_t*>(a.blocks) + (row_ok ? doc : 0) * (uint64_t)a.qpv;
+        auto word_at = [&](uint32_t wi) -> uint64_t { return (row_ok && wi < a.qpv) ? __ldg(words + wi) : 0ull; };
+        // K-block kb = words 2 kb, 2 kb + 1; two K-blocks of words in flight
+        uint64_t w0 = word_at(0), w1 = word_at(1), w2 = word_at(2), w3 = word_at(3);
+        for (uint32_t kb = 0; kb < n_kb; kb++, it++) {
+          const uint64_t lo = w0, hi = w1;
+          w0 = w2;
+          w1 = w3;
+          w2 = word_at(2 * kb + 4);
+          w3 = word_at(2 * kb + 5);
+          const uint32_t s = (uint32_t)(it % kPStages);
+          if (!acquire(s)) {
+            ok = false;
+            break;
+          }
+          const uint32_t base = smem_u32(S.a[s]) + a_row;
+#pragma unroll
+          for (uint32_t c = 0; c < 8; c++) {  // 16 coordinates per 16-byte chunk
+            const uint32_t h = (uint32_t)((c < 4 ? lo : hi) >> (16 * (c & 3)));
+            uint32_t o[4];
+#pragma unroll
+            for (uint32_t i = 0; i < 4; i++)  // 4 bits -> 4 bytes (the shifted copies never overlap)
+              o[i] = (((h >> (4 * i)) & 15u) * 0x00204081u) & 0x01010101u;
+            st_shared_v4(base + ((c ^ (r & 7)) << 4), o[0], o[1], o[2], o[3]);
+          }
+          publish(s);
+        }
+      } else {
+        const bool row_valid = pb < n_blocks;
+        const uint8_t* row_codes = a.blocks + pb * (uint64_t)a.pairs_pad * 16 + (uint64_t)(r & 31) * 16;
+        const uint32_t n_groups = n_kb / 4;  // one 16-byte code load covers 4 K-blocks
+        uint4 next = row_valid ? load_codes(row_codes) : make_uint4(0, 0, 0, 0);
+        for (uint32_t gi = 0; gi < n_groups && ok; gi++) {
+          const uint4 chunk = next;
+          if (row_valid && gi + 1 < n_groups) next = load_codes(row_codes + (uint64_t)(gi + 1) * 512);
+#pragma unroll
+          for (uint32_t j = 0; j < 4; j++) {
+            const uint32_t s = (uint32_t)(it % kPStages);
+            if (!acquire(s)) {
+              ok = false;
+              break;
+            }
+            const uint32_t w = j == 0 ? chunk.x : j == 1 ? chunk.y : j == 2 ? chunk.z : chunk.w;
+            const uint32_t base = smem_u32(S.a[s]) + a_row;
+#pragma unroll
+            for (uint32_t c = 0; c < 8; c++) {
+              const uint32_t sh = c == 0 ? (w << 3) & 0x78u : (w >> (4 * c - 3)) & 0x78u;  // 8 * nibble c
+              st_shared_v4(base + ((c ^ (r & 7)) << 4), shl1(sh), shl1(sh - 32), shl1(sh - 64), shl1(sh - 96));
+            }
+            publish(s);
+            it++;
+          }
+        }
+      }
+    }
+  } else {
+    // ---- epilogue (both CTAs) -------------------------------------------------------
+    const uint32_t e = (uint32_t)warp - 2 - kPBuildWarps;  // 0..15
+    const uint32_t et = (uint32_t)t - 32 * (2 + kPBuildWarps);
+    const uint32_t lq = (uint32_t)warp & 3, cq = e >> 2;  // lane quarter, column quarter
+    const uint32_t row = lq * 32 + lane;
+    const uint32_t acc_empty0 = peer_addr(smem_u32(&S.acc_empty[0]), 0);
+    uint2* list = S.list[e];
+    uint32_t lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    uint32_t tcount = 0;
+    for (uint64_t tile = cluster; tile < total; tile += n_clusters, tcount++) {
+      const uint64_t dt = tile / g.q_tiles, q0 = (tile % g.q_tiles) * nt;
+      const uint32_t nqt = (uint32_t)((a.nq - q0) < nt ? (a.nq - q0) : nt);
+      const uint32_t b = tcount & 1;
+      // per-query parameters of this tile (the previous tile's slot passes are done)
+      epi_sync();
+      if (et == 0) {
+        S.seg_full = 0;
+        S.any_exact = 0;
+      }
+      {
+        const uint32_t i = et;  // one query per epilogue thread (nt <= 256)
+        const bool v = i < nqt;
+        if (i < kPMaxN) {
+          S.bias[i] = (MODE == 0 && v) ? a.bias[q0 + i] : 0.0f;
+          S.invq[i] = (MODE == 0 && v) ? a.invq[q0 + i] : 0.0f;
+          S.thr[i] = (v && !dense) ? a.thr[(q0 + i) * a.thr_stride] : 0u;
+          S.cnt[i] = 0;
+          uint32_t am;
+          if (!v)
+            am = kNeverPasses;
+          else if (dense)
+            am = 0;
+          else if (MODE == 0)
+            am = filter_amin(S.bias[i], S.invq[i], a.inv_norm, S.thr[i], 255u * a.pairs_pad);
+          else {
+            am = bm_amin(a, S.thr[i]);
+            if (a.thr_pos) {  // (key, doc) <= (thr, tdoc): tie level by this CTA's doc range
+              const uint32_t p = a.thr_pos[(q0 + i) * a.thr_stride];
+              const uint64_t td = ((uint64_t)(p >> 5) * a.smp_stride) * 32 + (p & 31);
+              const uint64_t first = dt * 256 + rank * kPRows;
+              S.tdoc[i] = (uint32_t)td;
+              S.thr[i] = am;
+              am = td >= first + kPRows - 1 ? am : td < first ? am + 1 : kExactCompare;
+            }
+          }
+          S.amin[i] = am;
+        }
+      }
+      epi_sync();
+      for (uint32_t i = et; i < kPMaxN; i += kPEpiThreads)
+        if (S.amin[i] == kExactCompare) atomicOr(&S.any_exact, 1u);
+      // wait for the accumulator; one verdict for all epilogue warps
+      bool ready = false;
+      if (lane == 0) ready = !aborted(S) && mbar_wait_cluster(&S.acc_full[b], (tcount >> 1) & 1);
+      ready = __shfl_sync(0xFFFFFFFFu, ready, 0);
+      if (!ready && lane == 0) {
+        if (!aborted(S)) raise_abort(S, a.err);
+        atomicExch(&S.epi_stop, 1u);
+      }
+      epi_sync();
+      if (*reinterpret_cast<volatile uint32_t*>(&S.epi_stop)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint64_t pb = (dt * 8 + rank * 4 + lq) * a.block_stride;
+      const uint64_t doc = pb * 32 + lane;
+      const uint64_t u = dt * 256 + rank * kPRows + row;
+      const bool valid = pb < n_blocks && doc < a.n;
+      const uint32_t taddr = tmem + ((lq * 32) << 16) + b * 256;
+      const bool any_exact = S.any_exact != 0;
+      uint32_t wcount = 0;
+      for (uint32_t c = 0; c < 2; c++) {
+        const uint32_t cb = cq * 64 + c * 32;
+        if (cb >= nt) break;  // warp-uniform
+        uint32_t v[32];
+        __syncwarp();
+        tmem_ld32(taddr + cb, v);
+        if (dense) {
+#pragma unroll
+          for (uint32_t j = 0; j < 32; j++) {
+            const uint32_t q = cb + j;
+            if (valid && q < nqt)
+              a.keys[(q0 + q) * a.ld + u] =
+                  MODE == 0 ? desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm)) : bm_key(a, v[j]);
+          }
+          continue;
+        }
+        uint32_t hm = 0;  // queries this lane's doc passes
+        if (!any_exact) {
+#pragma unroll
+          for (uint32_t j = 0; j < 32; j += 4) {
+            const uint4 am = *reinterpret_cast<const uint4*>(&S.amin[cb + j]);
+            hm |= ((uint32_t)(v[j] >= am.x) << j) | ((uint32_t)(v[j + 1] >= am.y) << (j + 1)) |
+                  ((uint32_t)(v[j + 2] >= am.z) << (j + 2)) | ((uint32_t)(v[j + 3] >= am.w) << (j + 3));
+          }
+        } else {
+#pragma unroll
+          for (uint32_t j = 0; j < 32; j++) {
+            const uint32_t q = cb + j;
+            const uint32_t am = S.amin[q];
+            bool pass;
+            if (am != kExactCompare)
+              pass = v[j] >= am;
+            else if (MODE == 0)
+              pass = desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm)) <= S.thr[q];
+            else
+              pass = v[j] > S.thr[q] || (v[j] == S.thr[q] && doc <= S.tdoc[q]);
+            hm |= (uint32_t)pass << j;
+          }
+        }
+        if (!valid) hm = 0;
+        while (__any_sync(0xFFFFFFFFu, hm != 0)) {
+          const bool has = hm != 0;
+          const uint32_t j = has ? (uint32_t)(__ffs(hm) - 1) : 0u;
+          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+          const uint32_t pos = wcount + __popc(bal & lt);
+          if (has && pos < kPSegCap) {
+            uint32_t acc = v[0];
+#pragma unroll
+            for (uint32_t jj = 1; jj < 32; jj++) acc = jj == j ? v[jj] : acc;
+            list[pos] = make_uint2(acc, (cb + j) | (row << 16));
+          }
+          wcount += __popc(bal);
+          hm &= hm - 1;
+        }
+      }
+      // the accumulator is in registers / the list: release it to the MMA
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) arrive_remote(acc_empty0 + 8 * b);
+      if (!dense) {
+        // slots within each query's share of the tile, one global atomic per
+        // query per tile, then each warp writes its segment
+        const uint32_t tot = wcount < kPSegCap ? wcount : kPSegCap;
+        if (wcount > kPSegCap && lane == 0) atomicExch(&S.seg_full, 1u);
+        __syncwarp();
+        for (uint32_t j = lane; j < tot; j += 32) {
+          const uint32_t y = list[j].y;
+          list[j].y = y | (atom_add_shared(&S.cnt[y & 255], 1u) << 8);  // slot < 256
+        }
+        epi_sync();
+        if (et < nqt) {
+          if (S.seg_full)  // some kept doc did not fit: mark every query (bit 31 > cap)
+            atomicOr(&a.cnt[q0 + et], 0x80000000u);
+          else if (S.cnt[et])
+            S.base[et] = atomicAdd(&a.cnt[q0 + et], S.cnt[et]);
+        }
+        epi_sync();
+        for (uint32_t j = lane; j < tot; j += 32) {
+          const uint2 en = list[j];
+          const uint32_t q = en.y & 255, li = (en.y >> 8) & 255, rw = en.y >> 16;
+          const uint32_t pos = S.base[q] + li;
+          if (pos < a.cap) {
+            a.f_keys[(q0 + q) * a.cap + pos] =
+                MODE == 0 ? desc_key(tc_score(en.x, S.bias[q], S.invq[q], a.inv_norm)) : bm_key(a, en.x);
+            const uint64_t rpb = (dt * 8 + rank * 4 + (rw >> 5)) * a.block_stride;
+            a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw & 31));
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  cluster_sync_all();  // neither CTA frees the pair's tensor memory while the other uses it
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kPTmemCols) : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+    fastscan_pair_kernel(const __grid_constant__ CUtensorMap b_map, const TcArgs a, const PairGrid g) {
+  pair_body<0>(b_map, a, g);
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+    bitmap_pair_kernel(const __grid_constant__ CUtensorMap b_map, const TcArgs a, const PairGrid g) {
+  pair_body<1>(b_map, a, g);
+}
+
+// clusters of two that can be resident at once (each CTA takes a whole SM)
+uint32_t resident_pairs(const void* kernel, size_t smem) {
+  static std::mutex mu;
+  static int cached[2] = {0, 0};
+  const int slot = kernel == (const void*)fastscan_pair_kernel ? 0 : 1;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!cached[slot]) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2, 1, 1);
+    cfg.blockDim = dim3(kPThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kernel, &cfg) != cudaSuccess || n < 1) {
+      cudaGetLastError();
+      int dev = 0, sms = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      n = sms / 2 > 0 ? sms / 2 : 1;
+    }
+    cached[slot] = n;
+  }
+  return (uint32_t)cached[slot];
+}
+
+}  // namespace
+
+// Default: the bitmap family on pairs (1-CTA form epilogue-bound: measured
+// 22 % faster on pairs), FastScan on one CTA per tile (both forms are bound by
+// the MMA rate there, and the 1-CTA form keeps the tensor pipe busier).
+bool tc_pair_enabled(int mode) {
+  const char* e = getenv("OVB_TC_PAIR");
+  if (e && e[0] == '0') return false;
+  if (e && e[0] == '1') return true;
+  return mode == 1;
+}
+
+template <int MODE>
+void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream) {
+  if (!a.n || !a.nq) return;
+  const char* what = MODE == 0 ? "FastScan tensor-core scan" : "bitmap tensor-core scan";
+  const uint64_t k_bytes = (uint64_t)a.n_kb * kPKBytes;
+  if (!a.n_kb || (MODE == 0 && a.n_kb % 4)) throw std::invalid_argument(std::string(what) + ": bad K extent");
+  a.nt = a.nq >= kPMaxN ? kPMaxN : (uint32_t)((a.nq + 15) / 16 * 16);  // a multiple of 16 in [16, 256]
+  CUtensorMap map;
+  cuuint64_t gdim[2] = {(cuuint64_t)k_bytes, (cuuint64_t)a.nq};
+  cuuint64_t gstride[1] = {(cuuint64_t)k_bytes};
+  cuuint32_t box[2] = {(cuuint32_t)kPKBytes, (cuuint32_t)(a.nt / 2)};
+  cuuint32_t estride[2] = {1, 1};
+  CUresult rc = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)b_rows, gdim, gstride, box, estride,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (rc != CUDA_SUCCESS) throw CudaError(std::string("cuTensorMapEncodeTiled failed: ") + what);
+  if (MODE == 0 && 255ull * a.pairs_pad >= (1ull << 23)) throw std::invalid_argument(std::string(what) + ": dim too large");
+  if (MODE == 1 && (64ull * a.qpv >= (1ull << 24) || 2ull * a.n_kb < a.qpv))
+    throw std::invalid_argument(std::string(what) + ": row too long");
+  if (!a.keys && a.block_stride != 1) throw std::invalid_argument(std::string(what) + ": filter needs stride 1");
+  auto kernel = MODE == 0 ? fastscan_pair_kernel : bitmap_pair_kernel;
+  const size_t smem = sizeof(PSmem) + 1024;
+  OVB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const uint64_t n_blocks = (a.n + 31) / 32;
+  const uint64_t logical_blocks = (n_blocks + a.block_stride - 1) / a.block_stride;
+  PairGrid g;
+  const uint64_t doc_tiles = (logical_blocks + 7) / 8;
+  const uint64_t q_tiles = (a.nq + a.nt - 1) / a.nt;
+  if (doc_tiles > 0xFFFFFFFFull || q_tiles > 0xFFFFFFFFull || a.n >= (1ull << 32))
+    throw std::invalid_argument(std::string(what) + ": too many tiles");
+  g.n_doc_tiles = (uint32_t)doc_tiles;
+  g.q_tiles = (uint32_t)q_tiles;
+  const uint64_t total = doc_tiles * q_tiles;
+  uint64_t clusters = resident_pairs((const void*)kernel, smem);
+  if (clusters > total) clusters = total;
+  kernel<<<(unsigned)(2 * clusters), kPThreads, smem, stream>>>(map, a, g);
+  launched();
+}
+
+template void launch_tc_pair<0>(TcArgs, const uint8_t*, cudaStream_t);
+template void launch_tc_pair<1>(TcArgs, const uint8_t*, cudaStream_t);
+
+}  // namespace ovb

@@ -621,6 +621,46 @@ def test_bitmap_tensor_core_top_m_is_exact(orc, monkeypatch, dim, n_top, n, nq, 
     assert np.array_equal(fs.indices, ds.indices) and np.array_equal(fs.scores, ds.scores)
 
 
+@pytest.mark.parametrize("kind", ["fastscan", "bitmap", "multibucket"])
+def test_cta_pair_scan_matches_single_cta(monkeypatch, kind):
+    """The persistent CTA-pair tensor-core kernel (cta_group::2, double-buffered
+    accumulators) and the one-CTA-per-tile kernel give identical results, on
+    the sampled threshold pass, the filter and the dense key matrix, with a
+    partial last query tile and a partial last doc tile."""
+    n, nq = 70_001, 300
+    dim = 256 if kind == "fastscan" else 768
+    docs = ob.synth_docs(71, n, dim)
+    queries, _ = ob.synth_queries(71, n, nq, dim)
+    if kind == "fastscan":
+        ix = ob.RankQuantFastscan(dim)
+        ix.add(docs)
+        run = lambda: ix.search(queries, 333)
+    elif kind == "bitmap":
+        ix = ob.Bitmap(dim, 192)
+        ix.add(docs)
+        run = lambda: ix.search(queries, 500)
+    else:
+        ix = ob.MultiBucketBitmap(dim, 2)
+        ix.add(docs)
+        w = np.eye(4, dtype=np.float32).ravel()
+        run = lambda: np.array(ix.top_m_bilinear_batched(queries, w, 500))
+    monkeypatch.setenv("OVB_FASTSCAN_TC", "1")
+    monkeypatch.setenv("OVB_BITMAP_TC", "1")
+    out = {}
+    for pair in ("0", "1"):
+        for filt in ("0", "1"):
+            monkeypatch.setenv("OVB_TC_PAIR", pair)
+            monkeypatch.setenv("OVB_FASTSCAN_FILTER", filt)
+            out[(pair, filt)] = run()
+    base = out[("0", "0")]
+    for key, got in out.items():
+        if kind == "multibucket":
+            assert np.array_equal(got, base), key
+        else:
+            assert np.array_equal(got.indices, base.indices), key
+            assert np.array_equal(got.scores.view(np.uint32), base.scores.view(np.uint32)), key
+
+
 def test_bitmap_tensor_core_duplicate_rows(orc, monkeypatch):
     """400 distinct rows tiled 100x: every key level holds >= 100 docs, so the
     tie bound alone decides which equal-key docs the filter keeps."""
