@@ -351,8 +351,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-rate", type=float, default=150_000.0, help="offered queries/s")
-    ap.add_argument("--mixed-queries", type=int, default=0,
-                    help="also run the mixed-k/bits batch (N=1M, dim 1024) with this many queries; 0 = skip")
+    ap.add_argument("--mixed-queries", type=int, default=-1,
+                    help="also run the mixed-k/bits batch (N=1M, dim 1024) with this many queries; "
+                         "0 = skip, -1 = 4096 on a single GPU")
     ap.add_argument("--large", default="auto", choices=["auto", "on", "off"],
                     help="also run the N=10M dim-768 bitmap / multi-bucket configuration (auto: one GPU only)")
     args = ap.parse_args()
@@ -367,6 +368,7 @@ def main():
     from ordvec_b200.replicas import ReplicaGroup, rank_env, shard_seed, whole_job_rate
 
     rank, world, local = rank_env()
+    mixed_q = args.mixed_queries if args.mixed_queries >= 0 else (4096 if world == 1 else 0)
     torch.cuda.set_device(local)
     ob.set_device(local)
     dev = torch.device("cuda", local)
@@ -511,7 +513,7 @@ def main():
                   "p99_ms": float(np.percentile(plain_ms, 99)), "queries": P, "launches_per_query": plain_launches,
                   "identical_top10_vs_batched": identical, "batched_over_plain": value / world / plain_qps},
         "serving": serving,
-        "mixed_batch": mixed_run(ob, args.mixed_queries, args.steps) if args.mixed_queries > 0 else None,
+        "mixed_batch": mixed_run(ob, mixed_q, args.steps) if mixed_q > 0 else None,
         "large_corpus": large_run(ob, torch, dev, args.steps, args.plain_queries)
         if args.large == "on" or (args.large == "auto" and world == 1) else None,
         "stages_ms": dict(zip(STAGES, stages)),

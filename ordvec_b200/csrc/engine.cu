@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <vector>
 
 #include "ovb_host.h"
 
@@ -231,6 +232,64 @@ bool use_rank_tc(const Index& rq, uint64_t nq) {
   return nq >= 64 && rq.n >= 4096;
 }
 
+// Split-BF16 filter for rows of kp candidates: the sample-threshold plan with
+// kp in place of m (OVB_SPLIT_FILTER=0 disables).
+static bool split_filter_plan(uint64_t n, uint64_t kp, FilterPlan& fp) {
+  const char* e = getenv("OVB_SPLIT_FILTER");
+  if (e && e[0] == '0') return false;
+  return kp <= kSelectSmemCap && filter_plan(n, (uint32_t)kp, fp);
+}
+
+static uint64_t split_filter_bytes_per_query(const FilterPlan& fp, uint64_t kp) {
+  return fp.n_s * 4 + (uint64_t)fp.r * 8 + (uint64_t)fp.cap * 8 + 4 + kp * 12 + 8;
+}
+
+// Enqueues the filtered split-BF16 pipeline for qn queries (no host
+// synchronisation, graph-capturable): sample scan, each query's r-th sample
+// key as threshold, filtered scan, top-kp of the kept docs by split score,
+// margin test, FP64 rescoring of the kp, top-ke into out_keys / out_ids.
+// *d_flag |= 1 when some query kept fewer than kp or more than cap docs, or
+// its kp-th split score is within twice the error bound of its k-th: the
+// result is then not known to be exact and the caller redoes the rows.
+// Kept sets are prefixes of the split-key order, so their top-kp is the
+// whole index's.
+static void split_filtered(const Index& rq, const uint16_t* qs, const float* qu, const float* l1, uint64_t qn, uint32_t ke,
+                    uint32_t kp, const FilterPlan& fp, uint32_t q_per_tile, uint32_t* d_flag, uint32_t* out_keys,
+                    uint32_t* out_ids, Workspace& w, cudaStream_t st) {
+  const uint64_t n = rq.n;
+  const uint32_t dim = rq.dim, bits = rq.bits, id_bits = bits_for(n - 1);
+  const uint8_t* codes = rq.codes.as<uint8_t>();
+  const float inv_norm = inv_rankquant_norm(dim, bits);
+  uint32_t* err = w.tc_err_word(st);
+  uint32_t* smp = (uint32_t*)w.smp_keys.ensure(qn * fp.n_s * 4);
+  launch_rank_scan_tc(codes, n, dim, bits, qs, qn, inv_norm, fp.stride, smp, fp.n_s, q_per_tile, err, st);
+  uint32_t* tk = (uint32_t*)w.thr_keys.ensure(qn * fp.r * 4);
+  uint32_t* ti = (uint32_t*)w.thr_ids.ensure(qn * fp.r * 4);
+  select_rows(w, smp, nullptr, nullptr, fp.n_s, fp.n_s, qn, fp.r, 32, bits_for(fp.n_s - 1), tk, ti, st);
+  w.mark(st, 6);
+  uint32_t* cnt = (uint32_t*)w.f_cnt.ensure(qn * 4);
+  uint32_t* fk = (uint32_t*)w.f_keys.ensure(qn * fp.cap * 4);
+  uint32_t* fi = (uint32_t*)w.f_ids.ensure(qn * fp.cap * 4);
+  OVB_CUDA(cudaMemsetAsync(cnt, 0, qn * 4, st));
+  launch_rank_filter_tc(codes, n, dim, bits, qs, qn, inv_norm, tk + (fp.r - 1), fp.r, cnt, fp.cap, fk, fi, q_per_tile,
+                        err, st);
+  launch_filter_check(cnt, qn, kp, fp.cap, d_flag, st);
+  w.mark(st, 2);
+  uint32_t* ck = (uint32_t*)w.sel_keys.ensure(qn * kp * 4);
+  uint32_t* ci = (uint32_t*)w.sel_ids.ensure(qn * kp * 4);
+  select_rows(w, fk, fi, nullptr, fp.cap, fp.cap, qn, kp, 32, id_bits, ck, ci, st, cnt);
+  launch_clamp_ids(ci, qn * kp, (uint32_t)n, st);  // a row that kept < kp docs ends in sentinels
+  launch_split_margin(ck, qn, kp, ke, l1, split_error_bound(dim, bits, inv_norm), d_flag, st);
+  w.mark(st, 3);
+  uint64_t* off = (uint64_t*)w.off.ensure((qn + 1) * 8);
+  launch_uniform_offsets(off, qn, kp, st);
+  uint32_t* k2 = (uint32_t*)w.keys2.ensure(qn * kp * 4);
+  launch_asym_subset(codes, dim, bits, qu, qn, off, ci, kp, inv_norm, k2, st);
+  w.mark(st, 4);
+  select_rows(w, k2, ci, off, 0, 0, qn, ke, 32, id_bits, out_keys, out_ids, st);
+  w.mark(st, 5);
+}
+
 uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t nq, uint64_t k, bool exact,
                                      Workspace& w, cudaStream_t st, uint32_t q_per_tile) {
   require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "search_asymmetric");
@@ -248,17 +307,41 @@ uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t
   launch_split_queries(qu, nq, dim, qs, l1, st);
   uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
   uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
-  uint64_t qc = keys_budget() / (n * 4);
-  if (qc < 1) qc = 1;
-  if (qc > nq) qc = nq;
-  uint32_t* keys = (uint32_t*)w.keys.ensure(qc * n * 4);
   uint32_t* flag = (uint32_t*)w.f_flag.ensure(4);
   uint32_t* flag_h = (uint32_t*)w.f_flag_host.ensure(4);
   const uint32_t id_bits = bits_for(n - 1);
   w.split_kp = 0;
+  const uint64_t kp0 = std::min<uint64_t>(std::max<uint64_t>(2ull * ke, ke + 64ull), n);
+  FilterPlan fp;
+  // rows that passed the filtered pipeline; the others take the key matrix below
+  std::vector<char> done;
+  if (exact && split_filter_plan(n, kp0, fp)) {
+    uint64_t fc = keys_budget() / split_filter_bytes_per_query(fp, kp0);
+    if (fc < 1) fc = 1;
+    done.assign(nq, 0);
+    for (uint64_t q0 = 0; q0 < nq; q0 += fc) {
+      const uint64_t qn = nq - q0 < fc ? nq - q0 : fc;
+      OVB_CUDA(cudaMemsetAsync(flag, 0, 4, st));
+      split_filtered(rq, qs + q0 * 2 * dim, qu + q0 * dim, l1 + q0, qn, ke, (uint32_t)kp0, fp, q_per_tile, flag,
+                     ok + q0 * ke, oi + q0 * ke, w, st);
+      OVB_CUDA(cudaMemcpyAsync(flag_h, flag, 4, cudaMemcpyDeviceToHost, st));
+      OVB_CUDA(cudaStreamSynchronize(st));
+      if (!*flag_h) {
+        std::fill(done.begin() + q0, done.begin() + q0 + qn, 1);
+        w.split_kp = std::max<uint64_t>(w.split_kp, kp0);
+      }
+    }
+  }
+  uint64_t qc = keys_budget() / (n * 4);
+  if (qc < 1) qc = 1;
+  if (qc > nq) qc = nq;
+  uint32_t* keys = nullptr;
   for (uint64_t q0 = 0; q0 < nq; q0 += qc) {
     const uint64_t qn = nq - q0 < qc ? nq - q0 : qc;
-    launch_rank_scan_tc(rq.codes.as<uint8_t>(), n, dim, bits, qs + q0 * 2 * dim, qn, inv_norm, keys, n,
+    if (!done.empty() && std::all_of(done.begin() + q0, done.begin() + q0 + qn, [](char c) { return c != 0; }))
+      continue;
+    if (!keys) keys = (uint32_t*)w.keys.ensure(qc * n * 4);
+    launch_rank_scan_tc(rq.codes.as<uint8_t>(), n, dim, bits, qs + q0 * 2 * dim, qn, inv_norm, 1, keys, n,
                         q_per_tile, w.tc_err_word(st), st);
     w.mark(st, 2);
     if (!exact) {
@@ -295,24 +378,40 @@ uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t
   return ke;
 }
 
+bool split_fixed_fits(const Index& rq, uint64_t nq, uint64_t k) {
+  const uint64_t n = rq.n, ke = k < n ? k : n;
+  const uint64_t kp = std::min<uint64_t>(std::max<uint64_t>(2 * ke, ke + 64), n);
+  FilterPlan fp;
+  if (split_filter_plan(n, kp, fp) && nq * split_filter_bytes_per_query(fp, kp) <= keys_budget()) return true;
+  return nq * n * 4 <= keys_budget();
+}
+
 uint32_t engine_rankquant_split_fixed(const Index& rq, const float* d_q, uint64_t nq, uint64_t k, uint64_t kp,
                                       uint32_t q_per_tile, uint32_t* d_flag, Workspace& w, cudaStream_t st) {
   require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "search_asymmetric");
   const uint64_t n = rq.n;
   const uint32_t ke = (uint32_t)(k < n ? k : n);
   if (!ke || !nq) return ke;
-  if (!rank_tc_eligible(rq.dim, rq.bits) || nq * n * 4 > keys_budget())
-    fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "fixed split search: shape outside the single-chunk form");
   if (kp > n) kp = n;
   if (kp < ke) kp = ke;
+  FilterPlan fp;
+  const bool filtered = split_filter_plan(n, kp, fp) && nq * split_filter_bytes_per_query(fp, kp) <= keys_budget();
+  if (!rank_tc_eligible(rq.dim, rq.bits) || (!filtered && nq * n * 4 > keys_budget()))
+    fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "fixed split search: shape outside the single-chunk form");
   const uint32_t dim = rq.dim, bits = rq.bits, id_bits = bits_for(n - 1);
   const float* qu = normalised(w, d_q, nq, dim, st);
   const float inv_norm = inv_rankquant_norm(dim, bits);
   uint16_t* qs = (uint16_t*)w.q_split.ensure(nq * 2 * dim * 2);
   float* l1 = (float*)w.q_l1.ensure(nq * 4);
   launch_split_queries(qu, nq, dim, qs, l1, st);
+  uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
+  uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
+  if (filtered) {
+    split_filtered(rq, qs, qu, l1, nq, ke, (uint32_t)kp, fp, q_per_tile, d_flag, ok, oi, w, st);
+    return ke;
+  }
   uint32_t* keys = (uint32_t*)w.keys.ensure(nq * n * 4);
-  launch_rank_scan_tc(rq.codes.as<uint8_t>(), n, dim, bits, qs, nq, inv_norm, keys, n, q_per_tile,
+  launch_rank_scan_tc(rq.codes.as<uint8_t>(), n, dim, bits, qs, nq, inv_norm, 1, keys, n, q_per_tile,
                       w.tc_err_word(st), st);
   uint32_t* tk = (uint32_t*)w.thr_keys.ensure(nq * kp * 4);
   uint32_t* ti = (uint32_t*)w.thr_ids.ensure(nq * kp * 4);
@@ -322,8 +421,7 @@ uint32_t engine_rankquant_split_fixed(const Index& rq, const float* d_q, uint64_
   launch_uniform_offsets(off, nq, (uint32_t)kp, st);
   uint32_t* k2 = (uint32_t*)w.keys2.ensure(nq * kp * 4);
   launch_asym_subset(rq.codes.as<uint8_t>(), dim, bits, qu, nq, off, ti, kp, inv_norm, k2, st);
-  select_rows(w, k2, ti, off, 0, 0, nq, ke, 32, id_bits, (uint32_t*)w.out_keys.ensure(nq * ke * 4),
-              (uint32_t*)w.out_ids.ensure(nq * ke * 4), st);
+  select_rows(w, k2, ti, off, 0, 0, nq, ke, 32, id_bits, ok, oi, st);
   return ke;
 }
 

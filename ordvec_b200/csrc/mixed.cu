@@ -71,6 +71,7 @@ uint32_t autotune_tile(Plan& p) {
   Workspace& w = *p.w;
   const Index& ix = *p.ix;
   const uint64_t rows = std::min<uint64_t>(ix.n, 65536);
+  uint32_t* keys = (uint32_t*)w.keys.ensure(p.nq * rows * 4);  // tuning scans write rows x nq keys
   const float inv_norm = inv_norm_of(ix.dim, ix.bits);
   cudaEvent_t e0, e1;
   OVB_CUDA(cudaEventCreate(&e0));
@@ -79,12 +80,12 @@ uint32_t autotune_tile(Plan& p) {
   float best_ms = std::numeric_limits<float>::infinity();
   for (uint32_t qpt : {32u, 64u, 128u}) {
     if (qpt > 32 && (uint64_t)qpt / 2 >= p.nq) break;  // larger tiles than the batch change nothing
-    launch_rank_scan_tc(ix.codes.as<uint8_t>(), rows, ix.dim, ix.bits, w.q_split.p, p.nq, inv_norm,
-                        w.keys.as<uint32_t>(), ix.n, qpt, w.tc_err_word(w.stream), w.stream);
+    launch_rank_scan_tc(ix.codes.as<uint8_t>(), rows, ix.dim, ix.bits, w.q_split.p, p.nq, inv_norm, 1, keys, rows,
+                        qpt, w.tc_err_word(w.stream), w.stream);
     OVB_CUDA(cudaEventRecord(e0, w.stream));
     for (int r = 0; r < 2; r++)
-      launch_rank_scan_tc(ix.codes.as<uint8_t>(), rows, ix.dim, ix.bits, w.q_split.p, p.nq, inv_norm,
-                          w.keys.as<uint32_t>(), ix.n, qpt, w.tc_err_word(w.stream), w.stream);
+      launch_rank_scan_tc(ix.codes.as<uint8_t>(), rows, ix.dim, ix.bits, w.q_split.p, p.nq, inv_norm, 1, keys, rows,
+                          qpt, w.tc_err_word(w.stream), w.stream);
     OVB_CUDA(cudaEventRecord(e1, w.stream));
     OVB_CUDA(cudaEventSynchronize(e1));
     float ms = 0.0f;
@@ -208,7 +209,7 @@ bool mixed_plan_info(const Index& ix, uint64_t nq, uint64_t k, uint32_t* qpt, ui
 uint32_t mixed_group(const Index& ix, const float* h_q, uint64_t nq, uint64_t k, float* h_s, int64_t* h_i) {
   const uint32_t ke = (uint32_t)std::min<uint64_t>(k, ix.n);
   if (!ke || !nq) return ke;
-  if (graphs_enabled() && rank_tc_eligible(ix.dim, ix.bits) && nq * ix.n * 4 <= engine_keys_budget()) {
+  if (graphs_enabled() && rank_tc_eligible(ix.dim, ix.bits) && split_fixed_fits(ix, nq, k)) {
     Plan& p = plan_for(ix, nq, ke);
     std::lock_guard<std::mutex> lk(p.mu);
     run_plan(p, h_q, h_s, h_i);

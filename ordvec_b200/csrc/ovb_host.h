@@ -160,6 +160,8 @@ uint32_t engine_two_stage(const Index& rq, const Index& s1, const float* d_q, ui
                           uint64_t m, uint64_t k, Workspace& w, cudaStream_t st);
 uint64_t default_candidate_count(uint64_t k, uint64_t space);
 uint64_t engine_keys_budget();  // bytes a key matrix chunk may take
+// engine_rankquant_split_fixed can run nq queries of top-k in one chunk
+bool split_fixed_fits(const Index& rq, uint64_t nq, uint64_t k);
 
 // mixed batches (mixed.cu): drop the cached plans of an index that is freed or
 // grows; plan facts for tests and tools

@@ -109,10 +109,19 @@ float split_error_bound(uint32_t dim, uint32_t bits, float inv_norm);
 // q_unit rows -> [2 nq x dim] bf16 (row 2i = hi, 2i+1 = lo) and |q|_1 per row
 void launch_split_queries(const float* q_unit, uint64_t nq, uint32_t dim, void* out_bf16, float* l1,
                           cudaStream_t stream);
-// keys[q][doc] (ld) = desc key of the split-BF16 score; q_per_tile 0 = default
+// keys[q][u] (ld) = desc key of the split-BF16 score of logical doc u; with
+// block_stride > 1 only every block_stride-th 32-doc block is scored (u = the
+// sampled doc's position, fastscan_tc_sample_docs columns); q_per_tile 0 = default
 void launch_rank_scan_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_t bits, const void* q_split,
-                         uint64_t nq, float inv_norm, uint32_t* keys, uint64_t ld, uint32_t q_per_tile, uint32_t* err,
-                         cudaStream_t stream);
+                         uint64_t nq, float inv_norm, uint32_t block_stride, uint32_t* keys, uint64_t ld,
+                         uint32_t q_per_tile, uint32_t* err, cudaStream_t stream);
+// Threshold filter: appends (key32, doc) with key32 <= thr[q * thr_stride] to
+// row q of f_keys / f_ids (capacity cap); cnt[q] (zeroed by the caller) counts
+// every qualifying doc (bit 31 set when a tile's list overflowed).
+void launch_rank_filter_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_t bits, const void* q_split,
+                           uint64_t nq, float inv_norm, const uint32_t* thr, uint64_t thr_stride, uint32_t* cnt,
+                           uint32_t cap, uint32_t* f_keys, uint32_t* f_ids, uint32_t q_per_tile, uint32_t* err,
+                           cudaStream_t stream);
 // flag |= 1 if some row's kp-th key is not below its k-th minus twice the bound
 void launch_split_margin(const uint32_t* sel_keys, uint64_t nq, uint32_t kp, uint32_t k, const float* l1,
                          float bound_per_l1, uint32_t* flag, cudaStream_t stream);
@@ -139,6 +148,8 @@ void launch_finite_flag(const float* x, uint64_t count, uint32_t* flag, cudaStre
 
 // helper: key32 -> float score / sentinel mapping and uniform offsets
 void launch_uniform_offsets(uint64_t* off, uint64_t nq, uint64_t m, cudaStream_t stream);
+// ids[i] >= n (sentinels of underfull select rows) -> 0, so a gather stays in bounds
+void launch_clamp_ids(uint32_t* ids, uint64_t count, uint32_t n, cudaStream_t stream);
 void launch_keys_to_results(const uint32_t* keys, const uint32_t* ids, uint64_t count,
                             int mode, uint32_t n_top, float* scores, int64_t* out_ids,
                             cudaStream_t stream);

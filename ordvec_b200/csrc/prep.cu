@@ -268,6 +268,21 @@ void launch_finite_flag(const float* x, uint64_t count, uint32_t* flag, cudaStre
   launched();
 }
 
+namespace {
+__global__ void clamp_ids_kernel(uint32_t* ids, uint64_t count, uint32_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x)
+    if (ids[i] >= n) ids[i] = 0;
+}
+}  // namespace
+
+void launch_clamp_ids(uint32_t* ids, uint64_t count, uint32_t n, cudaStream_t stream) {
+  if (!count) return;
+  uint64_t blocks = ceil_div(count, 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  clamp_ids_kernel<<<(unsigned)blocks, 256, 0, stream>>>(ids, count, n);
+  launched();
+}
+
 void launch_uniform_offsets(uint64_t* off, uint64_t nq, uint64_t m, cudaStream_t stream) {
   uniform_offsets_kernel<<<ceil_div(nq + 1, 256), 256, 0, stream>>>(off, nq, m);
   launched();

@@ -47,9 +47,16 @@ constexpr uint32_t kRtBStage = kRtMaxN * kRtKBytes;
 constexpr uint32_t kRtTmemCols = 512;
 constexpr uint32_t kRtAcc1Col = 256;
 
+constexpr uint32_t kRtMaxQ = kRtMaxN / 2;  // queries per tile
+// filter list (key, q | slot << 8 | row << 16) in the dead A stages, one segment per epilogue warp
+constexpr uint32_t kRtSegCap = kRtStages * kRtAStage / 8 / (kRtBuilders / 32);
+
 struct RtSmem {
   uint8_t a[kRtStages][kRtAStage];
   uint8_t b[kRtStages][kRtBStage];
+  uint32_t thr[kRtMaxQ];
+  uint32_t cnt[kRtMaxQ];
+  uint32_t base[kRtMaxQ];
   uint64_t full_a[kRtStages];
   uint64_t full_b[kRtStages];
   uint64_t empty[kRtStages];
@@ -57,6 +64,7 @@ struct RtSmem {
   uint32_t tmem;
   uint32_t abort;
   uint32_t epi_ok;
+  uint32_t seg_full;
 };
 
 struct RtArgs {
@@ -66,9 +74,18 @@ struct RtArgs {
   uint32_t bpv;  // bytes per packed row
   uint64_t nq;
   uint32_t nt;  // B rows per tile (2 per query)
+  uint32_t block_stride;  // logical 32-doc block ub reads physical block ub * block_stride
   float inv_norm;
+  // dense output (keys != null): keys[q * ld + u], u = logical doc
   uint32_t* keys;
   uint64_t ld;
+  // filter output: (key, doc) with key <= thr[q * thr_stride] appended to row q
+  const uint32_t* thr;
+  uint64_t thr_stride;
+  uint32_t* cnt;
+  uint32_t cap;
+  uint32_t* f_keys;
+  uint32_t* f_ids;
   uint32_t* err;
 };
 
@@ -131,7 +148,11 @@ __global__ void __launch_bounds__(kRtThreads, 1)
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const uint32_t nt = a.nt;
   const uint64_t r0 = (uint64_t)blockIdx.y * nt;  // first B row of the tile
+  const uint64_t qb = r0 / 2;                     // first query of the tile
+  const uint32_t nqt = (uint32_t)((a.nq - qb) < nt / 2 ? (a.nq - qb) : nt / 2);
   const uint32_t n_kb = a.dim / 64;
+  const uint64_t n_blocks = (a.n + 31) / 32;
+  const bool dense = a.keys != nullptr;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
@@ -148,7 +169,12 @@ __global__ void __launch_bounds__(kRtThreads, 1)
     mbar_init(&S.acc_full, 1);
     S.abort = 0;
     S.epi_ok = 1;
+    S.seg_full = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (uint32_t i = t; i < kRtMaxQ; i += kRtThreads) {
+    S.thr[i] = (!dense && i < nqt) ? a.thr[(qb + i) * a.thr_stride] : 0u;
+    S.cnt[i] = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -211,8 +237,9 @@ __global__ void __launch_bounds__(kRtThreads, 1)
     {
       uint32_t t0, t1;
       nibble_table<BITS>((uint32_t)lane, t0, t1);
-      const uint64_t doc = (uint64_t)blockIdx.x * kRtM + r;
-      const bool valid = doc < a.n;
+      const uint64_t pb = ((uint64_t)blockIdx.x * 8 + (r >> 5)) * a.block_stride;
+      const uint64_t doc = pb * 32 + (r & 31);
+      const bool valid = pb < n_blocks && doc < a.n;
       // this thread's 4 * BITS code bytes of each K-block (8 * BITS bytes per K-block row)
       const uint8_t* rc = a.codes + (valid ? doc : 0) * (uint64_t)a.bpv + hc * 4 * BITS;
       const uint32_t a_row = smem_u32(S.a[0]) + (r >> 7) * kRtAHalf + ((r & 127) >> 3) * 1024 + (r & 7) * 128;
@@ -298,22 +325,82 @@ __global__ void __launch_bounds__(kRtThreads, 1)
       const uint32_t eg = (uint32_t)(warp - 2) >> 2;
       const uint32_t h = eg & 1, c0 = (eg >> 1) * 32, lq = (uint32_t)warp & 3;
       const uint32_t row = h * 128 + lq * 32 + lane;
-      const uint64_t doc = (uint64_t)blockIdx.x * kRtM + row;
-      const bool valid = doc < a.n;
+      const uint64_t pb = ((uint64_t)blockIdx.x * 8 + (row >> 5)) * a.block_stride;
+      const uint64_t doc = pb * 32 + lane;
+      const uint64_t u = (uint64_t)blockIdx.x * kRtM + row;
+      const bool valid = pb < n_blocks && doc < a.n;
       const uint32_t taddr = tmem + ((lq * 32) << 16) + h * kRtAcc1Col;
+      // filter list segment of this warp in the dead A stages
+      uint2* list = reinterpret_cast<uint2*>(&S.a[0][0]) + (uint32_t)(warp - 2) * kRtSegCap;
+      uint32_t wcount = 0;
+      uint32_t lt;
+      asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
       for (uint32_t cb = c0; cb < nt; cb += 64) {
         uint32_t v[32];
         __syncwarp();
         tmem_ld32(taddr + cb, v);
-        if (valid) {
+        uint32_t key[16];
 #pragma unroll
-          for (uint32_t p = 0; p < 16; p++) {
-            const uint64_t q = (r0 + cb) / 2 + p;
-            if (q < a.nq) {
-              const float sc =
-                  __fmul_rn(__fadd_rn(__uint_as_float(v[2 * p]), __uint_as_float(v[2 * p + 1])), a.inv_norm);
-              a.keys[q * a.ld + doc] = desc_key(sc);
+        for (uint32_t p = 0; p < 16; p++)
+          key[p] = desc_key(__fmul_rn(__fadd_rn(__uint_as_float(v[2 * p]), __uint_as_float(v[2 * p + 1])), a.inv_norm));
+        if (dense) {
+          if (valid) {
+#pragma unroll
+            for (uint32_t p = 0; p < 16; p++) {
+              const uint64_t q = qb + cb / 2 + p;
+              if (q < a.nq) a.keys[q * a.ld + u] = key[p];
             }
+          }
+          continue;
+        }
+        // filter: mask of the 16 queries this lane's doc passes, then ballot-ranked appends
+        uint32_t hm = 0;
+#pragma unroll
+        for (uint32_t p = 0; p < 16; p++) {
+          const uint32_t qi = cb / 2 + p;
+          hm |= (uint32_t)(qi < nqt && key[p] <= S.thr[qi]) << p;
+        }
+        if (!valid) hm = 0;
+        while (__any_sync(0xFFFFFFFFu, hm != 0)) {
+          const bool has = hm != 0;
+          const uint32_t p = has ? (uint32_t)(__ffs(hm) - 1) : 0u;
+          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+          const uint32_t pos = wcount + __popc(bal & lt);
+          if (has && pos < kRtSegCap) {
+            uint32_t kk = key[0];
+#pragma unroll
+            for (uint32_t pp = 1; pp < 16; pp++) kk = pp == p ? key[pp] : kk;
+            list[pos] = make_uint2(kk, (cb / 2 + p) | (row << 16));
+          }
+          wcount += __popc(bal);
+          hm &= hm - 1;
+        }
+      }
+      if (!dense) {
+        const uint32_t total = wcount < kRtSegCap ? wcount : kRtSegCap;
+        if (wcount > kRtSegCap && lane == 0) atomicExch(&S.seg_full, 1u);
+        __syncwarp();
+        for (uint32_t e = lane; e < total; e += 32) {
+          const uint32_t y = list[e].y;
+          list[e].y = y | (atom_add_shared(&S.cnt[y & 255], 1u) << 8);  // slot < 256
+        }
+        rt_epi_bar();
+        const uint32_t i = (uint32_t)t - 64;
+        if (i < nqt) {
+          if (S.seg_full)  // some kept doc did not fit: bit 31 makes the count exceed any cap
+            atomicOr(&a.cnt[qb + i], 0x80000000u);
+          else if (S.cnt[i])
+            S.base[i] = atomicAdd(&a.cnt[qb + i], S.cnt[i]);
+        }
+        rt_epi_bar();
+        for (uint32_t e = lane; e < total; e += 32) {
+          const uint2 en = list[e];
+          const uint32_t q = en.y & 255, li = (en.y >> 8) & 255, rw = en.y >> 16;
+          const uint32_t pos = S.base[q] + li;
+          if (pos < a.cap) {
+            a.f_keys[(qb + q) * a.cap + pos] = en.x;
+            const uint64_t rpb = ((uint64_t)blockIdx.x * 8 + (rw >> 5)) * a.block_stride;
+            a.f_ids[(qb + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw & 31));
           }
         }
       }
@@ -390,29 +477,20 @@ void launch_split_margin(const uint32_t* sel_keys, uint64_t nq, uint32_t kp, uin
   launched();
 }
 
-void launch_rank_scan_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_t bits, const void* q_split,
-                         uint64_t nq, float inv_norm, uint32_t* keys, uint64_t ld, uint32_t q_per_tile, uint32_t* err,
-                         cudaStream_t stream) {
-  if (!n || !nq) return;
-  if (!rank_tc_eligible(dim, bits)) throw std::invalid_argument("rank tensor-core scan: dim must be a multiple of 64");
-  RtArgs a{};
-  a.codes = codes;
-  a.n = n;
-  a.dim = dim;
-  a.bpv = dim * bits / 8;
-  a.nq = nq;
+static void launch_rank_tc(RtArgs a, uint32_t bits, const void* q_split, uint32_t q_per_tile, cudaStream_t stream) {
+  if (!a.n || !a.nq) return;
+  if (!rank_tc_eligible(a.dim, bits)) throw std::invalid_argument("rank tensor-core scan: dim must be a multiple of 64");
+  a.bpv = a.dim * bits / 8;
+  if (!a.block_stride) a.block_stride = 1;
+  if (!a.keys && a.block_stride != 1) throw std::invalid_argument("rank tensor-core scan: filter needs stride 1");
   uint32_t qt = q_per_tile ? q_per_tile : 128;  // queries per tile: 8..128, multiple of 8
   if (qt > 128) qt = 128;
-  if ((uint64_t)qt > nq) qt = (uint32_t)nq;
+  if ((uint64_t)qt > a.nq) qt = (uint32_t)a.nq;
   qt = (qt + 7) / 8 * 8;
   a.nt = 2 * qt;
-  a.inv_norm = inv_norm;
-  a.keys = keys;
-  a.ld = ld;
-  a.err = err;
   CUtensorMap map;
-  cuuint64_t gdim[2] = {(cuuint64_t)dim, (cuuint64_t)(2 * nq)};
-  cuuint64_t gstride[1] = {(cuuint64_t)dim * 2};
+  cuuint64_t gdim[2] = {(cuuint64_t)a.dim, (cuuint64_t)(2 * a.nq)};
+  cuuint64_t gstride[1] = {(cuuint64_t)a.dim * 2};
   cuuint32_t box[2] = {64, a.nt};
   cuuint32_t estride[2] = {1, 1};
   CUresult rc = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(q_split), gdim, gstride,
@@ -420,9 +498,11 @@ void launch_rank_scan_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (rc != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed for the split query matrix");
   const size_t smem = sizeof(RtSmem) + 1024;
-  const uint64_t doc_tiles = (n + kRtM - 1) / kRtM;
-  const uint64_t q_tiles = (2 * nq + a.nt - 1) / a.nt;
-  if (q_tiles > 65535 || doc_tiles > 0x7FFFFFFF)
+  const uint64_t n_blocks = (a.n + 31) / 32;
+  const uint64_t logical_blocks = (n_blocks + a.block_stride - 1) / a.block_stride;
+  const uint64_t doc_tiles = (logical_blocks + 7) / 8;
+  const uint64_t q_tiles = (2 * a.nq + a.nt - 1) / a.nt;
+  if (q_tiles > 65535 || doc_tiles > 0x7FFFFFFF || a.n >= (1ull << 32))
     throw std::invalid_argument("rank tensor-core scan: grid too large; split the query batch");
   dim3 grid((unsigned)doc_tiles, (unsigned)q_tiles);
 #define OVB_RT(B)                                                                                              \
@@ -438,6 +518,43 @@ void launch_rank_scan_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_
     OVB_RT(4);
 #undef OVB_RT
   launched();
+}
+
+void launch_rank_scan_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_t bits, const void* q_split,
+                         uint64_t nq, float inv_norm, uint32_t block_stride, uint32_t* keys, uint64_t ld,
+                         uint32_t q_per_tile, uint32_t* err, cudaStream_t stream) {
+  RtArgs a{};
+  a.codes = codes;
+  a.n = n;
+  a.dim = dim;
+  a.nq = nq;
+  a.block_stride = block_stride;
+  a.inv_norm = inv_norm;
+  a.keys = keys;
+  a.ld = ld;
+  a.err = err;
+  launch_rank_tc(a, bits, q_split, q_per_tile, stream);
+}
+
+void launch_rank_filter_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_t bits, const void* q_split,
+                           uint64_t nq, float inv_norm, const uint32_t* thr, uint64_t thr_stride, uint32_t* cnt,
+                           uint32_t cap, uint32_t* f_keys, uint32_t* f_ids, uint32_t q_per_tile, uint32_t* err,
+                           cudaStream_t stream) {
+  RtArgs a{};
+  a.codes = codes;
+  a.n = n;
+  a.dim = dim;
+  a.nq = nq;
+  a.block_stride = 1;
+  a.inv_norm = inv_norm;
+  a.thr = thr;
+  a.thr_stride = thr_stride;
+  a.cnt = cnt;
+  a.cap = cap;
+  a.f_keys = f_keys;
+  a.f_ids = f_ids;
+  a.err = err;
+  launch_rank_tc(a, bits, q_split, q_per_tile, stream);
 }
 
 }  // namespace ovb

@@ -97,3 +97,20 @@ def test_mixed_batch_other_shapes_and_errors():
     with pytest.raises(ob.OrdvecError) as e:
         ob.mixed_plan_info(a, 40, 5)  # never planned
     assert e.value.status == 2
+
+
+def test_mixed_batch_filtered_plans(monkeypatch):
+    """At N large enough for the split-BF16 threshold filter the captured plans
+    run the filtered pipeline; results equal the key-matrix plans'."""
+    docs, queries, indices, sel, ks = _setup(dim=256, n=150_000, nq=400, seed=0x0DD5EED7)
+    got = ob.search_mixed(indices, sel, ks, queries)
+    again = ob.search_mixed(indices, sel, ks, queries)  # graph replay
+    assert np.array_equal(again.indices, got.indices)
+    monkeypatch.setenv("OVB_SPLIT_FILTER", "0")
+    monkeypatch.setenv("OVB_MIXED_GRAPH", "0")
+    dense = ob.search_mixed(indices, sel, ks, queries)
+    assert np.array_equal(dense.indices, got.indices)
+    assert np.array_equal(dense.scores.view(np.uint32), got.scores.view(np.uint32))
+    for j, rq in enumerate(indices):
+        rows = np.flatnonzero(sel == j)
+        assert ob.mixed_plan_info(rq, rows.size, int(ks[rows].max()))["replays"] >= 1

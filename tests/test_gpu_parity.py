@@ -325,6 +325,28 @@ def test_split_bf16_rank_scan(orc, monkeypatch, dim, bits, n):
     assert np.array_equal(a.indices, b.indices)
 
 
+@pytest.mark.parametrize("bits", [1, 2, 4])
+def test_split_bf16_threshold_filter(orc, monkeypatch, bits):
+    """Split-BF16 search through the sample-threshold filter (kept docs only,
+    no key matrix) returns the key-matrix path's exact top-k, and the oracle's."""
+    n, dim, nq = 120_000, 256, 200
+    docs = ob.synth_docs(83 + bits, n, dim)
+    queries, _ = ob.synth_queries(83 + bits, n, nq, dim)
+    rq = ob.RankQuant(dim, bits)
+    rq.add(docs)
+    packed = orc.rankquant_encode(docs, dim, bits)
+    for k in (10, 100):
+        filt = rq.search_asymmetric(queries, k)
+        monkeypatch.setenv("OVB_SPLIT_FILTER", "0")
+        dense = rq.search_asymmetric(queries, k)
+        monkeypatch.delenv("OVB_SPLIT_FILTER")
+        assert np.array_equal(filt.indices, dense.indices)
+        assert np.array_equal(filt.scores.view(np.uint32), dense.scores.view(np.uint32))
+        for qi in (0, nq - 1):
+            s64 = orc.rq_scores_f64(packed, n, dim, bits, queries[qi])
+            check_float_topk(filt.indices_for_query(qi), filt.scores_for_query(qi), np.arange(n), s64, k)
+
+
 def test_rankquant_large_k_uses_global_select(orc):
     dim, bits, n = 128, 2, 9000
     docs = ob.synth_docs(5, n, dim)
