@@ -339,6 +339,42 @@ def serving_run(ob, rq, fs, queries, batched_ids, seconds: float, rate_qps: floa
             "identical_top10_vs_batched": same[0]}
 
 
+# ------------------------------------------------------- profiling cases
+def profile_case(case: str):
+    """Small single-kernel workloads for ncu captures (no timing, no JSON):
+      bitmap    Bitmap(768, 192) top-2000 of 1024 queries, N=2M (bitmap_pair_kernel)
+      popc      the same index, one query per call (popc_rows_kernel, wide select)
+      rank      RankQuant(1024, 2) exact top-100 of 1024 queries, N=1M (rank_tc_kernel)
+      fastscan  this workload's FastScan top-1000 of 1000 queries (fastscan_tc_kernel)
+    Each search runs more than once so captures can skip the first call."""
+    import ordvec_b200 as ob
+
+    if case in ("bitmap", "popc"):
+        n = 2_000_000
+        bm = ob.Bitmap(768, 192)
+        for first in range(0, n, 1_000_000):
+            bm.add(ob.synth_docs(0x0DD5EED4, 1_000_000, 768, first=first))
+        q, _ = ob.synth_queries(0x0DD5EED5, n, 1024, 768)
+        for _ in range(2 if case == "bitmap" else 3):
+            bm.top_m_candidates_batched(q, 2000) if case == "bitmap" else bm.top_m_candidates(q[0], 2000)
+    elif case == "rank":
+        n = 1_000_000
+        rq = ob.RankQuant(1024, 2)
+        rq.add(ob.synth_docs(0x0DD5EED3, n, 1024))
+        q, _ = ob.synth_queries(0x0DD5EED4, n, 1024, 1024)
+        for _ in range(2):
+            rq.search_asymmetric(q, 100)
+    elif case == "fastscan":
+        fs = ob.RankQuantFastscan(DIM)
+        fs.add(ob.synth_docs(SEED, N_DOCS, DIM))
+        q, _ = ob.synth_queries(SEED + 1, N_DOCS, NQ, DIM)
+        for _ in range(2):
+            fs.search(q, M)
+    else:
+        raise SystemExit(f"unknown profile case {case}")
+    print(f"profile case {case}: done", flush=True)
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -356,7 +392,11 @@ def main():
                          "0 = skip, -1 = 4096 on a single GPU")
     ap.add_argument("--large", default="auto", choices=["auto", "on", "off"],
                     help="also run the N=10M dim-768 bitmap / multi-bucket configuration (auto: one GPU only)")
+    ap.add_argument("--profile-case", choices=["bitmap", "popc", "rank", "fastscan"],
+                    help="run one small kernel workload for an ncu capture and exit")
     args = ap.parse_args()
+    if args.profile_case:
+        return profile_case(args.profile_case)
     if args.impl == "reference":
         return reference_arm(args)
 
