@@ -198,6 +198,71 @@ def mixed_run(ob, nq: int, steps: int):
             "form": "host buffers; split-BF16 tcgen05 scan + exact FP64 rescoring; CUDA-graph replay"}
 
 
+# ------------------------------------------------------ sign -> b=1, plain
+def sign_plain_run(ob, torch, dev, plain_queries: int, cpu: bool):
+    """The sign-bitmap configuration the reference runs on CPU: N=100,000
+    synthetic docs (seed 0x0DD5EED1), dim 1024, SignBitmap top-320 (default
+    policy) -> RankQuant b=1 asymmetric rerank, k=10, one query per call
+    (device pointers, CUDA events per call), next to the batched form (1,000
+    queries in one call) and the CPU oracle (AVX-512 + OpenMP, all threads)."""
+    from oracle import oracle as orc
+
+    n, dim, seed, nq, k = 100_000, 1024, 0x0DD5EED1, 1000, 10
+    docs = ob.synth_docs(seed, n, dim)
+    queries, _ = ob.synth_queries(seed + 1, n, nq, dim)
+    sb, rq = ob.SignBitmap(dim), ob.RankQuant(dim, 1)
+    sb.add(docs)
+    rq.add(docs)
+    m = orc.policy_candidate_count(k, n)  # TwoStageCandidatePolicy default: 320 at k=10
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    d_q = torch.from_numpy(queries).to(dev)
+    d_s = torch.empty(nq * k, dtype=torch.float32, device=dev)
+    d_i = torch.empty(nq * k, dtype=torch.int64, device=dev)
+    run = lambda cnt, qp, s_, i_: ob.two_stage_search_device(rq, sb, qp, cnt, 0, k, s_, i_, sp)  # 0: policy
+    for _ in range(3):
+        run(nq, d_q.data_ptr(), d_s.data_ptr(), d_i.data_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    reps = 5
+    for _ in range(reps):
+        run(nq, d_q.data_ptr(), d_s.data_ptr(), d_i.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    batched_ms = e0.elapsed_time(e1) / reps
+    ids = d_i.view(nq, k).cpu().numpy()
+    P = min(max(plain_queries, 20), nq)
+    p_s = torch.empty(P * k, dtype=torch.float32, device=dev)
+    p_i = torch.empty(P * k, dtype=torch.int64, device=dev)
+    for qi in range(3):
+        run(1, d_q[qi].data_ptr(), p_s[qi * k:].data_ptr(), p_i[qi * k:].data_ptr())
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(P)]
+    for qi in range(P):
+        ev[qi][0].record(stream)
+        run(1, d_q[qi].data_ptr(), p_s[qi * k:].data_ptr(), p_i[qi * k:].data_ptr())
+        ev[qi][1].record(stream)
+    torch.cuda.synchronize(dev)
+    plain_ms = [a.elapsed_time(b) for a, b in ev]
+    out = {"workload": f"N={n} dim={dim}: SignBitmap top-{m} -> RankQuant b=1 rerank top-{k}",
+           "plain_qps": 1e3 / statistics.mean(plain_ms), "plain_p50_ms": float(np.percentile(plain_ms, 50)),
+           "plain_p99_ms": float(np.percentile(plain_ms, 99)), "plain_queries": P,
+           "plain_launches_per_query": ob.last_launch_count(),
+           "batched_qps": nq / (batched_ms * 1e-3), "batched_ms": batched_ms,
+           "identical_top10_plain_vs_batched": bool(np.array_equal(p_i.view(P, k).cpu().numpy(), ids[:P]))}
+    if cpu:
+        words = orc.sign_encode(docs, dim)
+        packed = orc.rankquant_encode(docs, dim, 1)
+        threads = orc.max_threads()
+        sample = min(nq, 200)
+        orc.cpu_sign_two_stage(words, packed, n, dim, 1, queries[:8], m, k, threads)
+        t0 = time.perf_counter()
+        orc.cpu_sign_two_stage(words, packed, n, dim, 1, queries[:sample], m, k, threads)
+        dt = time.perf_counter() - t0
+        out["cpu_oracle"] = {"qps": sample / dt, "cores": threads, "sample": f"{sample} queries, one batch",
+                             "kind": "port (AVX-512 popcount + b1 LUT rerank)"}
+    return out
+
+
 # ------------------------------------------------------------- large corpus
 def large_run(ob, torch, dev, steps: int, plain_queries: int):
     """The large-corpus configuration: N=10,000,000 synthetic docs, dim 768,
@@ -386,7 +451,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
-    ap.add_argument("--serve-rate", type=float, default=150_000.0, help="offered queries/s")
+    ap.add_argument("--serve-rate", type=float, default=200_000.0, help="offered queries/s")
     ap.add_argument("--mixed-queries", type=int, default=-1,
                     help="also run the mixed-k/bits batch (N=1M, dim 1024) with this many queries; "
                          "0 = skip, -1 = 4096 on a single GPU")
@@ -554,6 +619,7 @@ def main():
                   "identical_top10_vs_batched": identical, "batched_over_plain": value / world / plain_qps},
         "serving": serving,
         "mixed_batch": mixed_run(ob, mixed_q, args.steps) if mixed_q > 0 else None,
+        "sign_b1_plain": sign_plain_run(ob, torch, dev, args.plain_queries, not args.no_cpu) if world == 1 else None,
         "large_corpus": large_run(ob, torch, dev, args.steps, args.plain_queries)
         if args.large == "on" or (args.large == "auto" and world == 1) else None,
         "stages_ms": dict(zip(STAGES, stages)),
