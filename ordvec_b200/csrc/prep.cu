@@ -256,7 +256,9 @@ void launch_bitmap_query(const float* q, uint64_t nq, uint32_t dim, uint32_t n_t
 void launch_fastscan_lut(const float* q_unit, uint64_t nq, uint32_t dim, uint32_t pairs_pad,
                          uint8_t* lut, float* bias_sum, float* inv_q, cudaStream_t stream) {
   if (!nq) return;
-  fastscan_lut_kernel<<<(unsigned)nq, 256, 0, stream>>>(q_unit, dim, pairs_pad, lut, bias_sum, inv_q);
+  // one CTA per query; a lone query (one-query calls) gets the widest CTA
+  fastscan_lut_kernel<<<(unsigned)nq, nq <= 16 ? 1024 : 256, 0, stream>>>(q_unit, dim, pairs_pad, lut, bias_sum,
+                                                                          inv_q);
   launched();
 }
 
