@@ -160,8 +160,9 @@ void filtered_select(Workspace& w, uint64_t n, uint64_t nq, uint32_t me, const F
   }
 }
 
-// Tensor-core overlap scan for constant-weight bitmaps and identity-weight
-// multi-bucket bitmaps, batches of at least 32 queries; OVB_BITMAP_TC=0/1 forces.
+// Tensor-core overlap scan for sign bitmaps (Hamming), constant-weight bitmaps
+// and identity-weight multi-bucket bitmaps, batches of at least 32 queries;
+// OVB_BITMAP_TC=0/1 forces.
 bool use_bitmap_tc(uint64_t nq) {
   const char* e = getenv("OVB_BITMAP_TC");
   if (e && e[0] == '0') return false;
@@ -170,21 +171,22 @@ bool use_bitmap_tc(uint64_t nq) {
 }
 
 // Stage-1 top-m of a bitmap-family index on the tensor cores: key_kind 0 for a
-// constant-weight bitmap, 1 for a multi-bucket bitmap with identity weights;
-// qb = query words (qpv per query).
+// constant-weight bitmap, 1 for a multi-bucket bitmap with identity weights,
+// 2 for a sign bitmap (Hamming); qb = query words (qpv per query).
 void bitmap_tc_candidates(const Index& s1, const uint64_t* qb, uint32_t qpv, uint32_t key_kind, uint32_t key_bits,
                           uint64_t nq, uint32_t me, uint32_t* sk, uint32_t* si, Workspace& w, cudaStream_t st) {
   const uint64_t n = s1.n;
   const uint64_t row = (uint64_t)bitmap_tc_kblocks(qpv) * 128;
   uint8_t* qx = (uint8_t*)w.lut.ensure(nq * row);
-  launch_bitmap_tc_query(qb, nq, qpv, qx, st);
+  uint32_t* qpop = key_kind == 2 ? (uint32_t*)w.bias.ensure(nq * 4) : nullptr;  // bias is FastScan's
+  launch_bitmap_tc_query(qb, nq, qpv, qx, qpop, st);
   const uint64_t* words = s1.codes.as<uint64_t>();
   uint32_t* err = w.tc_err_word(st);
   auto dense = [&](uint64_t qa, uint64_t qn) {
     full_scan_select(w, qn, n, me, key_bits, sk + qa * me, si + qa * me, st,
                      [&](uint64_t q0, uint64_t qm, uint32_t* keys) {
-                       launch_bitmap_scan_tc(words, n, qpv, key_kind, s1.n_top, qx + (qa + q0) * row, qm, 1, keys, n,
-                                             err, st);
+                       launch_bitmap_scan_tc(words, n, qpv, key_kind, s1.n_top, qpop ? qpop + qa + q0 : nullptr,
+                                             qx + (qa + q0) * row, qm, 1, keys, n, err, st);
                      });
   };
   FilterPlan fp;
@@ -196,12 +198,13 @@ void bitmap_tc_candidates(const Index& s1, const uint64_t* qb, uint32_t qpv, uin
   filtered_select(
       w, n, nq, me, fp, key_bits, sk, si, st,
       [&](uint64_t q0, uint64_t qn, uint32_t* smp) {
-        launch_bitmap_scan_tc(words, n, qpv, key_kind, s1.n_top, qx + q0 * row, qn, fp.stride, smp, fp.n_s, err, st);
+        launch_bitmap_scan_tc(words, n, qpv, key_kind, s1.n_top, qpop ? qpop + q0 : nullptr, qx + q0 * row, qn,
+                              fp.stride, smp, fp.n_s, err, st);
       },
       [&](uint64_t q0, uint64_t qn, const uint32_t* thr, const uint32_t* pos, uint32_t* cnt, uint32_t* fk,
           uint32_t* fi) {
-        launch_bitmap_filter_tc(words, n, qpv, key_kind, s1.n_top, qx + q0 * row, qn, thr, pos, fp.stride, fp.r, cnt,
-                                fp.cap, fk, fi, err, st);
+        launch_bitmap_filter_tc(words, n, qpv, key_kind, s1.n_top, qpop ? qpop + q0 : nullptr, qx + q0 * row, qn, thr,
+                                pos, fp.stride, fp.r, cnt, fp.cap, fk, fi, err, st);
       },
       dense);
 }
@@ -479,8 +482,8 @@ uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint6
         launch_bitmap_query(d_q, nq, s1.dim, s1.n_top, qb, st);
       w.mark(st, 1);
       const uint32_t key_bits = bits_for(mode == 0 ? s1.dim : s1.n_top);
-      if (mode == 1 && use_bitmap_tc(nq)) {
-        bitmap_tc_candidates(s1, qb, s1.qpv(), 0, key_bits, nq, me, sk, si, w, st);
+      if (use_bitmap_tc(nq)) {  // sign: Hamming (key kind 2); bitmap: n_top - overlap (0)
+        bitmap_tc_candidates(s1, qb, s1.qpv(), mode == 0 ? 2 : 0, key_bits, nq, me, sk, si, w, st);
         break;
       }
       w.mark(st, 6);  // no sampling stage

@@ -82,18 +82,21 @@ void launch_fastscan_filter_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs
 // Tensor-core bitmap overlap scan (same file, u8 x u8 -> s32 on 0/1 bytes).
 // Rows of qpv u64 words; key_kind 0: key32 = n_top - popcount(q AND d)
 // (constant-weight bitmap), 1: key32 = desc_key((float)popcount) (multi-bucket
-// with identity weights).  The query operand is the query bits expanded to
-// 0/1 bytes (launch_bitmap_tc_query), bitmap_tc_kblocks(qpv) * 128 per query.
+// with identity weights), 2: key32 = popcount(q XOR d) = |q| + |d| - 2 |q AND d|
+// (sign bitmap; qpop = |q| per query).  The query operand is the query bits
+// expanded to 0/1 bytes (launch_bitmap_tc_query, which also writes qpop when
+// given), bitmap_tc_kblocks(qpv) * 128 per query.
 uint32_t bitmap_tc_kblocks(uint32_t qpv);
-void launch_bitmap_tc_query(const uint64_t* qbits, uint64_t nq, uint32_t qpv, uint8_t* out, cudaStream_t stream);
+void launch_bitmap_tc_query(const uint64_t* qbits, uint64_t nq, uint32_t qpv, uint8_t* out, uint32_t* qpop,
+                            cudaStream_t stream);
 void launch_bitmap_scan_tc(const uint64_t* words, uint64_t n, uint32_t qpv, uint32_t key_kind, uint32_t n_top,
-                           const uint8_t* q_bytes, uint64_t nq, uint32_t block_stride, uint32_t* keys, uint64_t ld,
-                           uint32_t* err, cudaStream_t stream);
+                           const uint32_t* qpop, const uint8_t* q_bytes, uint64_t nq, uint32_t block_stride,
+                           uint32_t* keys, uint64_t ld, uint32_t* err, cudaStream_t stream);
 // Filter with a tie bound: keeps (key32, doc) <= (thr, tdoc) in (key, doc)
 // order, tdoc = the doc of sample position thr_pos[q * thr_stride] of a sample
 // taken with block stride smp_stride (every doc at key < thr when thr_pos is null).
 void launch_bitmap_filter_tc(const uint64_t* words, uint64_t n, uint32_t qpv, uint32_t key_kind, uint32_t n_top,
-                             const uint8_t* q_bytes, uint64_t nq, const uint32_t* thr, const uint32_t* thr_pos,
+                             const uint32_t* qpop, const uint8_t* q_bytes, uint64_t nq, const uint32_t* thr, const uint32_t* thr_pos,
                              uint32_t smp_stride, uint64_t thr_stride, uint32_t* cnt, uint32_t cap, uint32_t* f_keys,
                              uint32_t* f_ids, uint32_t* err, cudaStream_t stream);
 // *flag |= 1 when some cnt[q] < need or > cap.

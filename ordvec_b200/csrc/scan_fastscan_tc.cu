@@ -74,6 +74,7 @@ struct TcSmem {
   uint32_t thr[kTcMaxN];
   uint32_t amin[kTcMaxN];  // filter: smallest passing accumulator, or kExactCompare
   uint32_t tdoc[kTcMaxN];  // bitmap filter, tie level: last passing doc id
+  uint32_t qpop[kTcMaxN];  // sign bitmaps: query popcounts
   uint64_t full_a[kTcStages];
   uint64_t full_b[kTcStages];
   uint64_t empty[kTcStages];
@@ -143,6 +144,7 @@ __device__ __forceinline__ void tc_scan_body(const CUtensorMap& lut_map, const T
     S.bias[i] = (MODE == 0 && v) ? a.bias[q0 + i] : 0.0f;
     S.invq[i] = (MODE == 0 && v) ? a.invq[q0 + i] : 0.0f;
     S.thr[i] = (v && !dense) ? a.thr[(q0 + i) * a.thr_stride] : 0u;
+    S.qpop[i] = (MODE == 1 && v && a.key_kind == 2) ? a.qpop[q0 + i] : 0u;
     if (MODE == 0)
       S.amin[i] = !v ? kNeverPasses
                      : dense ? kExactCompare
@@ -153,7 +155,7 @@ __device__ __forceinline__ void tc_scan_body(const CUtensorMap& lut_map, const T
       // key <= thr  <=>  acc >= am.  With a tie bound, (key, doc) <= (thr, tdoc):
       // this tile's docs [first, first + 256) all pass the tie level, none do,
       // or the compare is per doc (kExactCompare, am kept in thr).
-      const uint32_t am = bm_amin(a, S.thr[i]);
+      const uint32_t am = bm_amin_q(a, S.qpop[i], S.thr[i]);
       S.amin[i] = am;
       if (a.thr_pos) {
         const uint32_t p = a.thr_pos[(q0 + i) * a.thr_stride];
@@ -377,6 +379,7 @@ __device__ __forceinline__ void tc_scan_body(const CUtensorMap& lut_map, const T
       const uint64_t doc = pb * 32 + lane;
       const uint64_t u = (uint64_t)blockIdx.x * kTcM + row;
       const bool valid = pb < n_blocks && doc < a.n;
+      const uint32_t dpop = (MODE == 1 && a.key_kind == 2) ? row_popcount(a, doc, valid) : 0u;
       const uint32_t taddr = tmem + ((lq * 32) << 16) + h * kAcc1Col;
       const bool any_exact = S.any_exact != 0;
       // filter list: the A stages are dead once acc_full has fired; each warp
@@ -390,13 +393,17 @@ __device__ __forceinline__ void tc_scan_body(const CUtensorMap& lut_map, const T
         uint32_t v[32];
         __syncwarp();
         tmem_ld32(taddr + cb, v);
+        if (MODE == 1 && a.key_kind == 2) {
+#pragma unroll
+          for (uint32_t j = 0; j < 32; j++) v[j] = ham_y(v[j], dpop);
+        }
         if (dense) {
 #pragma unroll
           for (uint32_t j = 0; j < 32; j++) {
             const uint32_t q = cb + j;
             if (valid && q < nqt)
               a.keys[(q0 + q) * a.ld + u] =
-                  MODE == 0 ? desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm)) : bm_key(a, v[j]);
+                  MODE == 0 ? desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm)) : bm_key_q(a, S.qpop[q], v[j]);
           }
           continue;
         }
@@ -468,7 +475,7 @@ __device__ __forceinline__ void tc_scan_body(const CUtensorMap& lut_map, const T
           const uint32_t pos = S.base[q] + li;
           if (pos < a.cap) {
             a.f_keys[(q0 + q) * a.cap + pos] =
-                MODE == 0 ? desc_key(tc_score(en.x, S.bias[q], S.invq[q], a.inv_norm)) : bm_key(a, en.x);
+                MODE == 0 ? desc_key(tc_score(en.x, S.bias[q], S.invq[q], a.inv_norm)) : bm_key_q(a, S.qpop[q], en.x);
             const uint64_t rpb = ((uint64_t)blockIdx.x * 8 + (rw >> 5)) * a.block_stride;
             a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw & 31));
           }
@@ -490,6 +497,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 __global__ void __launch_bounds__(kTcThreads, 1)
     bitmap_tc_kernel(const __grid_constant__ CUtensorMap q_map, const TcArgs a) {
   tc_scan_body<1>(q_map, a);
+}
+
+// popcount of each query's qpv words
+__global__ void query_popcount_kernel(const uint64_t* __restrict__ qbits, uint64_t nq, uint32_t qpv,
+                                      uint32_t* __restrict__ out) {
+  const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nq) return;
+  uint32_t c = 0;
+  for (uint32_t i = 0; i < qpv; i++) c += __popcll(qbits[q * qpv + i]);
+  out[q] = c;
 }
 
 // query bits (qpv u64 words per query) -> 0/1 bytes, row_bytes per query
@@ -610,16 +627,22 @@ void launch_fastscan_filter_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs
 
 uint32_t bitmap_tc_kblocks(uint32_t qpv) { return (qpv + 1) / 2; }
 
-void launch_bitmap_tc_query(const uint64_t* qbits, uint64_t nq, uint32_t qpv, uint8_t* out, cudaStream_t stream) {
+void launch_bitmap_tc_query(const uint64_t* qbits, uint64_t nq, uint32_t qpv, uint8_t* out, uint32_t* qpop,
+                            cudaStream_t stream) {
   if (!nq) return;
   const uint32_t row = bitmap_tc_kblocks(qpv) * kTcKBytes;
   uint64_t blocks = (nq * row + 255) / 256;
   if (blocks > 148 * 16) blocks = 148 * 16;
   expand_query_bits_kernel<<<(unsigned)blocks, 256, 0, stream>>>(qbits, nq, qpv, row, out);
   launched();
+  if (qpop) {
+    query_popcount_kernel<<<(unsigned)((nq + 255) / 256), 256, 0, stream>>>(qbits, nq, qpv, qpop);
+    launched();
+  }
 }
 
 void launch_bitmap_scan_tc(const uint64_t* words, uint64_t n, uint32_t qpv, uint32_t key_kind, uint32_t n_top,
+                           const uint32_t* qpop,
                            const uint8_t* q_bytes, uint64_t nq, uint32_t block_stride, uint32_t* keys, uint64_t ld,
                            uint32_t* err, cudaStream_t stream) {
   TcArgs a{};
@@ -628,6 +651,7 @@ void launch_bitmap_scan_tc(const uint64_t* words, uint64_t n, uint32_t qpv, uint
   a.qpv = qpv;
   a.n_kb = bitmap_tc_kblocks(qpv);
   a.key_kind = key_kind;
+  a.qpop = qpop;
   a.n_top = n_top;
   a.block_stride = block_stride ? block_stride : 1;
   a.nq = nq;
@@ -638,6 +662,7 @@ void launch_bitmap_scan_tc(const uint64_t* words, uint64_t n, uint32_t qpv, uint
 }
 
 void launch_bitmap_filter_tc(const uint64_t* words, uint64_t n, uint32_t qpv, uint32_t key_kind, uint32_t n_top,
+                           const uint32_t* qpop,
                              const uint8_t* q_bytes, uint64_t nq, const uint32_t* thr, const uint32_t* thr_pos,
                              uint32_t smp_stride, uint64_t thr_stride, uint32_t* cnt, uint32_t cap, uint32_t* f_keys,
                              uint32_t* f_ids, uint32_t* err, cudaStream_t stream) {
@@ -647,6 +672,7 @@ void launch_bitmap_filter_tc(const uint64_t* words, uint64_t n, uint32_t qpv, ui
   a.qpv = qpv;
   a.n_kb = bitmap_tc_kblocks(qpv);
   a.key_kind = key_kind;
+  a.qpop = qpop;
   a.n_top = n_top;
   a.block_stride = 1;
   a.nq = nq;

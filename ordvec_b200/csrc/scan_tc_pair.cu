@@ -74,6 +74,7 @@ struct PSmem {
   uint32_t thr[kPMaxN];
   uint32_t amin[kPMaxN];
   uint32_t tdoc[kPMaxN];
+  uint32_t qpop[kPMaxN];  // sign bitmaps: query popcounts
   uint32_t cnt[kPMaxN];
   uint32_t base[kPMaxN];
   uint64_t full_a[kPStages];
@@ -371,6 +372,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           S.bias[i] = (MODE == 0 && v) ? a.bias[q0 + i] : 0.0f;
           S.invq[i] = (MODE == 0 && v) ? a.invq[q0 + i] : 0.0f;
           S.thr[i] = (v && !dense) ? a.thr[(q0 + i) * a.thr_stride] : 0u;
+          S.qpop[i] = (MODE == 1 && v && a.key_kind == 2) ? a.qpop[q0 + i] : 0u;
           S.cnt[i] = 0;
           uint32_t am;
           if (!v)
@@ -380,7 +382,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           else if (MODE == 0)
             am = filter_amin(S.bias[i], S.invq[i], a.inv_norm, S.thr[i], 255u * a.pairs_pad);
           else {
-            am = bm_amin(a, S.thr[i]);
+            am = bm_amin_q(a, S.qpop[i], S.thr[i]);
             if (a.thr_pos) {  // (key, doc) <= (thr, tdoc): tie level by this CTA's doc range
               const uint32_t p = a.thr_pos[(q0 + i) * a.thr_stride];
               const uint64_t td = ((uint64_t)(p >> 5) * a.smp_stride) * 32 + (p & 31);
@@ -411,6 +413,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
       const uint64_t doc = pb * 32 + lane;
       const uint64_t u = dt * 256 + rank * kPRows + row;
       const bool valid = pb < n_blocks && doc < a.n;
+      const uint32_t dpop = (MODE == 1 && a.key_kind == 2) ? row_popcount(a, doc, valid) : 0u;
       const uint32_t taddr = tmem + ((lq * 32) << 16) + b * 256;
       const bool any_exact = S.any_exact != 0;
       uint32_t wcount = 0;
@@ -420,13 +423,17 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
         uint32_t v[32];
         __syncwarp();
         tmem_ld32(taddr + cb, v);
+        if (MODE == 1 && a.key_kind == 2) {
+#pragma unroll
+          for (uint32_t j = 0; j < 32; j++) v[j] = ham_y(v[j], dpop);
+        }
         if (dense) {
 #pragma unroll
           for (uint32_t j = 0; j < 32; j++) {
             const uint32_t q = cb + j;
             if (valid && q < nqt)
               a.keys[(q0 + q) * a.ld + u] =
-                  MODE == 0 ? desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm)) : bm_key(a, v[j]);
+                  MODE == 0 ? desc_key(tc_score(v[j], S.bias[q], S.invq[q], a.inv_norm)) : bm_key_q(a, S.qpop[q], v[j]);
           }
           continue;
         }
@@ -497,7 +504,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           const uint32_t pos = S.base[q] + li;
           if (pos < a.cap) {
             a.f_keys[(q0 + q) * a.cap + pos] =
-                MODE == 0 ? desc_key(tc_score(en.x, S.bias[q], S.invq[q], a.inv_norm)) : bm_key(a, en.x);
+                MODE == 0 ? desc_key(tc_score(en.x, S.bias[q], S.invq[q], a.inv_norm)) : bm_key_q(a, S.qpop[q], en.x);
             const uint64_t rpb = (dt * 8 + rank * 4 + (rw >> 5)) * a.block_stride;
             a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw & 31));
           }

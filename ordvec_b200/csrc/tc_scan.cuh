@@ -20,7 +20,8 @@ struct TcArgs {
   uint32_t pairs_pad;     // FastScan
   uint32_t qpv;           // bitmap: u64 words per row
   uint32_t n_top;         // bitmap: set bits per row (key = n_top - overlap)
-  uint32_t key_kind;      // bitmap: 0 key = n_top - acc, 1 key = desc_key((float)acc)
+  uint32_t key_kind;      // bitmap: 0 key = n_top - acc, 1 key = desc_key((float)acc), 2 Hamming
+  const uint32_t* qpop;   // bitmap key_kind 2: popcount of each query's words
   uint32_t n_kb;          // 128-byte K-blocks
   uint32_t block_stride;
   const float* bias;
@@ -106,6 +107,34 @@ __device__ inline uint32_t bm_amin(const TcArgs& a, uint32_t thr) {
       lo = mid + 1;
   }
   return lo;
+}
+
+// Sign bitmaps (key_kind 2): Hamming(q, d) = |q| + |d| - 2 |q AND d|.  The
+// epilogue compares y = 2 acc + kHamBias - |d| (per doc row) against
+// |q| + kHamBias - thr (per query), so the threshold test stays one compare
+// per (doc, query) and key <= thr <=> y >= that bound.
+constexpr uint32_t kHamBias = 1u << 20;
+
+__device__ __forceinline__ uint32_t ham_y(uint32_t acc, uint32_t dpop) { return 2 * acc + kHamBias - dpop; }
+
+// key of a (possibly transformed) accumulator for a query with popcount qpop
+__device__ __forceinline__ uint32_t bm_key_q(const TcArgs& a, uint32_t qpop, uint32_t y) {
+  return a.key_kind == 2 ? qpop + kHamBias - y : bm_key(a, y);
+}
+
+// smallest (transformed) accumulator whose key is <= thr
+__device__ __forceinline__ uint32_t bm_amin_q(const TcArgs& a, uint32_t qpop, uint32_t thr) {
+  return a.key_kind == 2 ? qpop + kHamBias - thr : bm_amin(a, thr);
+}
+
+// popcount of a bitmap row (qpv words), 0 for an invalid row
+__device__ __forceinline__ uint32_t row_popcount(const TcArgs& a, uint64_t doc, bool valid) {
+  uint32_t c = 0;
+  if (valid) {
+    const uint64_t* w = reinterpret_cast<const uint64_t*>(a.blocks) + doc * (uint64_t)a.qpv;
+    for (uint32_t i = 0; i < a.qpv; i++) c += __popcll(__ldg(w + i));
+  }
+  return c;
 }
 
 __device__ __forceinline__ uint4 load_codes(const uint8_t* p) {

@@ -643,7 +643,7 @@ def test_bitmap_tensor_core_top_m_is_exact(orc, monkeypatch, dim, n_top, n, nq, 
     assert np.array_equal(fs.indices, ds.indices) and np.array_equal(fs.scores, ds.scores)
 
 
-@pytest.mark.parametrize("kind", ["fastscan", "bitmap", "multibucket"])
+@pytest.mark.parametrize("kind", ["fastscan", "bitmap", "multibucket", "sign"])
 def test_cta_pair_scan_matches_single_cta(monkeypatch, kind):
     """The persistent CTA-pair tensor-core kernel (cta_group::2, double-buffered
     accumulators) and the one-CTA-per-tile kernel give identical results, on
@@ -661,6 +661,10 @@ def test_cta_pair_scan_matches_single_cta(monkeypatch, kind):
         ix = ob.Bitmap(dim, 192)
         ix.add(docs)
         run = lambda: ix.search(queries, 500)
+    elif kind == "sign":
+        ix = ob.SignBitmap(dim)
+        ix.add(docs)
+        run = lambda: np.array(ix.top_m_candidates_batched(queries, 500))
     else:
         ix = ob.MultiBucketBitmap(dim, 2)
         ix.add(docs)
@@ -676,11 +680,33 @@ def test_cta_pair_scan_matches_single_cta(monkeypatch, kind):
             out[(pair, filt)] = run()
     base = out[("0", "0")]
     for key, got in out.items():
-        if kind == "multibucket":
+        if kind in ("multibucket", "sign"):
             assert np.array_equal(got, base), key
         else:
             assert np.array_equal(got.indices, base.indices), key
             assert np.array_equal(got.scores.view(np.uint32), base.scores.view(np.uint32)), key
+
+
+@pytest.mark.parametrize("dim,n,nq,m", [(1024, 100_000, 64, 320), (384, 70_001, 300, 700), (192, 40_000, 40, 500)])
+def test_sign_tensor_core_top_m_is_exact(orc, monkeypatch, dim, n, nq, m):
+    """Sign-bitmap Hamming candidates from the tensor-core overlap scan
+    (|q| + |d| - 2 |q AND d|, sampled threshold with the tie bound, and the
+    dense key matrix) equal the CUDA-core XOR-popcount scan and the oracle."""
+    docs = ob.synth_docs(89, n, dim)
+    queries, _ = ob.synth_queries(89, n, nq, dim)
+    sb = ob.SignBitmap(dim)
+    sb.add(docs)
+    f, d, c = _bitmap_modes(monkeypatch, lambda: np.array(sb.top_m_candidates_batched(queries, m)), **_BITMAP_THREE)
+    assert np.array_equal(f, d) and np.array_equal(f, c)
+    words = orc.sign_encode(docs, dim)
+    for qi in (0, nq - 1):
+        assert np.array_equal(f[qi], orc.sign_top_m(words, n, dim, queries[qi], m)), qi
+    rq = ob.RankQuant(dim, 1)
+    rq.add(docs)
+    a, b = _bitmap_modes(monkeypatch, lambda: ob.two_stage_search(rq, sb, queries, 0, 10),
+                         tc={"OVB_BITMAP_TC": "1"}, cuda_core={"OVB_BITMAP_TC": "0"})
+    assert np.array_equal(a.indices, b.indices)
+    assert np.array_equal(a.scores.view(np.uint32), b.scores.view(np.uint32))
 
 
 def test_bitmap_tensor_core_duplicate_rows(orc, monkeypatch):
