@@ -440,6 +440,104 @@ def profile_case(case: str):
     print(f"profile case {case}: done", flush=True)
 
 
+# ------------------------------------------------------ serving, 3 indices
+def serving_multi_run(ob, seconds: float, rates):
+    """The serving configuration: three device-resident indices -- (dim 384,
+    N=2M, b=1), (768, 5M, b=2), (1024, 1M, b=4) -- each behind a sign-bitmap
+    stage 1 (two-stage route, default candidate policy), seeded Poisson request
+    streams offering each rate in `rates` queries/s with 1-256 queries per
+    request, k in {10, 50, 100} and a uniformly drawn index; ob.Server with 3
+    workers (continuous batching, HBM-budget admission).  Per rate: completed
+    QPS and request latency p50/p99.  Beside it the plain per-request form (one
+    request at a time through ob.two_stage_search) and whether sampled
+    requests' answers in the mix equal their answers alone."""
+    import threading
+
+    specs = [(384, 2_000_000, 1), (768, 5_000_000, 2), (1024, 1_000_000, 4)]
+    seed = 0x0DD5EED5
+    t0 = time.perf_counter()
+    routes, pools = [], []
+    srv = ob.Server(workers=3, max_batch=1024)
+    keep = []
+    for j, (dim, n, bits) in enumerate(specs):
+        rq, sb = ob.RankQuant(dim, bits), ob.SignBitmap(dim)
+        for first in range(0, n, 1_000_000):
+            d = ob.synth_docs(seed + j, min(1_000_000, n - first), dim, first=first)
+            rq.add(d)
+            sb.add(d)
+        q, _ = ob.synth_queries(seed + 16 + j, n, 2048, dim)
+        pools.append(q)
+        routes.append(srv.add_route(rq, sb))
+        keep.append((rq, sb))
+    build_s = time.perf_counter() - t0
+    srv.wait_ready()
+    rng = np.random.default_rng(seed)
+    out = {"workload": "3 indices: (384, 2M, b1), (768, 5M, b2), (1024, 1M, b4), each SignBitmap -> RankQuant; "
+                       "requests of 1-256 queries, k in {10,50,100}, seeded Poisson arrivals",
+           "build_s": build_s, "workers": 3, "rates": []}
+    sample_ans = {}
+    for rate in rates:
+        mean_size = 128.5
+        n_req = max(int(seconds * rate / mean_size), 16)
+        sizes = rng.integers(1, 257, n_req)
+        which = rng.integers(0, 3, n_req)
+        ks = rng.choice([10, 50, 100], n_req)
+        offs = rng.integers(0, 2048 - 256, n_req)
+        gaps = rng.exponential(mean_size / rate, n_req)
+        tickets, lat, done_at = [None] * n_req, [0.0] * n_req, [0.0] * n_req
+
+        def collect():
+            for i in range(n_req):
+                while tickets[i] is None:
+                    time.sleep(20e-6)
+                res, lat[i] = tickets[i].wait()
+                done_at[i] = time.perf_counter()
+                if i % 97 == 0:
+                    sample_ans[(rate, i)] = (int(which[i]), int(offs[i]), int(sizes[i]), int(ks[i]), res.indices.copy())
+
+        th = threading.Thread(target=collect)
+        th.start()
+        start = time.perf_counter()
+        due = start
+        for i in range(n_req):
+            due += gaps[i]
+            while time.perf_counter() < due:
+                pass
+            j, o, sz = int(which[i]), int(offs[i]), int(sizes[i])
+            tickets[i] = srv.submit(routes[j], pools[j][o:o + sz], int(ks[i]), 0)
+        th.join()
+        wall = max(done_at) - start
+        nq = int(sizes.sum())
+        out["rates"].append({"offered_qps": rate, "completed_qps": nq / wall, "requests": n_req, "queries": nq,
+                             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                             "mean_ms": float(np.mean(lat))})
+    st = srv.stats()
+    out["batches"], out["max_concurrent_batches"] = st["batches"], st["max_concurrent_batches"]
+    srv.close()
+    # plain per-request form: one request at a time, host buffers
+    rng2 = np.random.default_rng(seed + 1)
+    plain_lat, plain_q = [], 0
+    for i in range(120):
+        j, sz, k = int(rng2.integers(0, 3)), int(rng2.integers(1, 257)), int(rng2.choice([10, 50, 100]))
+        o = int(rng2.integers(0, 2048 - 256))
+        rq, sb = keep[j]
+        t1 = time.perf_counter()
+        ob.two_stage_search(rq, sb, pools[j][o:o + sz], 0, k)
+        plain_lat.append((time.perf_counter() - t1) * 1e3)
+        plain_q += sz
+    out["plain_per_request"] = {"qps": plain_q / (sum(plain_lat) * 1e-3), "p50_ms": float(np.percentile(plain_lat, 50)),
+                                "p99_ms": float(np.percentile(plain_lat, 99)), "requests": 120,
+                                "form": "one request at a time, ob.two_stage_search, host buffers"}
+    same = True
+    for (rate, i), (j, o, sz, k, ids) in list(sample_ans.items())[:24]:
+        rq, sb = keep[j]
+        alone = ob.two_stage_search(rq, sb, pools[j][o:o + sz], 0, k)
+        same &= bool(np.array_equal(alone.indices, ids))
+    out["identical_in_mix_vs_alone"] = same
+    out["checked_requests"] = min(len(sample_ans), 24)
+    return out
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -620,6 +718,8 @@ def main():
         "serving": serving,
         "mixed_batch": mixed_run(ob, mixed_q, args.steps) if mixed_q > 0 else None,
         "sign_b1_plain": sign_plain_run(ob, torch, dev, args.plain_queries, not args.no_cpu) if world == 1 else None,
+        "serving_multi": serving_multi_run(ob, args.serve_seconds, [20_000.0, 100_000.0, args.serve_rate])
+        if world == 1 and args.serve_seconds > 0 else None,
         "large_corpus": large_run(ob, torch, dev, args.steps, args.plain_queries)
         if args.large == "on" or (args.large == "auto" and world == 1) else None,
         "stages_ms": dict(zip(STAGES, stages)),
