@@ -102,7 +102,9 @@ bool filter_plan(uint64_t n, uint32_t m, FilterPlan& p) {
   const bool force = e && e[0] == '1';
   if (!m || !n || (!force && (n < 32768 || (uint64_t)m * 32 > n))) return false;
   uint32_t stride = 1;
-  while (stride < 64 && n / (2ull * stride) >= 8192) stride <<= 1;
+  // the sample pass costs about one CTA wave per 256 x 256 tile set, whatever
+  // the doc count, so the sample is kept near 4-8K docs (one wave at <= 256 queries)
+  while (stride < 64 && n / (2ull * stride) >= 4096) stride <<= 1;
   const uint64_t n_s = fastscan_tc_sample_docs(n, stride);
   const char* me = getenv("OVB_FASTSCAN_SAMPLE_MULT");
   const double mult = me ? strtod(me, nullptr) : 3.0;
