@@ -534,7 +534,7 @@ uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint6
           [&](uint64_t q0, uint64_t qn, const uint32_t* thr, const uint32_t*, uint32_t* cnt, uint32_t* fk,
               uint32_t* fi) {
             launch_fastscan_filter_tc(codes, n, s1.pairs_pad, lut + q0 * lut_row, bias + q0, invq + q0, inv_norm,
-                                      qn, thr, fp.r, cnt, fp.cap, fk, fi, err, st);
+                                      qn, thr, fp.r, cnt, fp.cap, fk, fi, (uint64_t)fp.r * n / fp.n_s, err, st);
           },
           dense_rows);
       break;

@@ -74,11 +74,13 @@ void launch_fastscan_scan_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_p
 uint64_t fastscan_tc_sample_docs(uint64_t n, uint32_t block_stride);
 // Threshold filter: appends (key32, doc) with key32 <= thr[q * thr_stride] to
 // row q of f_keys / f_ids (capacity cap); cnt[q] (zeroed by the caller) counts
-// every qualifying doc.
+// every qualifying doc.  expect_kept: the expected count per query (picks the
+// kernel form whose kept-entry lists fit it; 0 = unknown).
 void launch_fastscan_filter_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad, const uint8_t* lut,
                                const float* bias_sum, const float* inv_q, float inv_norm, uint64_t nq,
                                const uint32_t* thr, uint64_t thr_stride, uint32_t* cnt, uint32_t cap,
-                               uint32_t* f_keys, uint32_t* f_ids, uint32_t* err, cudaStream_t stream);
+                               uint32_t* f_keys, uint32_t* f_ids, uint64_t expect_kept, uint32_t* err,
+                               cudaStream_t stream);
 // Tensor-core bitmap overlap scan (same file, u8 x u8 -> s32 on 0/1 bytes).
 // Rows of qpv u64 words; key_kind 0: key32 = n_top - popcount(q AND d)
 // (constant-weight bitmap), 1: key32 = desc_key((float)popcount) (multi-bucket

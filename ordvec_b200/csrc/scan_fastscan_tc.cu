@@ -534,8 +534,16 @@ __global__ void filter_check_kernel(const uint32_t* __restrict__ cnt, uint64_t n
 template <int MODE>
 void launch_tc(TcArgs a, const uint8_t* b_rows, cudaStream_t stream) {
   if (!a.n || !a.nq) return;
-  if (tc_pair_enabled(MODE)) {
-    launch_tc_pair<MODE>(a, b_rows, stream);
+  TcForm form = tc_form(MODE);
+  if (form == TcForm::kPersist && !a.keys) {
+    // the persistent one-CTA form holds fewer kept entries per warp and tile
+    // than this form's (the dead A stages): use it when twice the expected
+    // share of a warp (32 docs x 128 queries) fits
+    const double per_warp = a.expect_kept ? (double)a.expect_kept * 32.0 / (double)a.n : 1e9;
+    if (2.0 * per_warp * 128.0 > (double)tc_persist_seg_cap()) form = TcForm::kTile;
+  }
+  if (form != TcForm::kTile) {
+    launch_tc_pair<MODE>(a, b_rows, stream, form == TcForm::kPair);
     return;
   }
   const char* what = MODE == 0 ? "FastScan tensor-core scan" : "bitmap tensor-core scan";
@@ -604,8 +612,10 @@ void launch_fastscan_scan_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_p
 void launch_fastscan_filter_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad, const uint8_t* lut,
                                const float* bias_sum, const float* inv_q, float inv_norm, uint64_t nq,
                                const uint32_t* thr, uint64_t thr_stride, uint32_t* cnt, uint32_t cap,
-                               uint32_t* f_keys, uint32_t* f_ids, uint32_t* err, cudaStream_t stream) {
+                               uint32_t* f_keys, uint32_t* f_ids, uint64_t expect_kept, uint32_t* err,
+                               cudaStream_t stream) {
   TcArgs a{};
+  a.expect_kept = expect_kept;
   a.blocks = blocks;
   a.n = n;
   a.pairs_pad = pairs_pad;

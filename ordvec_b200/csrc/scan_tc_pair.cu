@@ -56,19 +56,29 @@ constexpr int kPBuildWarps = 4;  // warps 2..5: one thread per doc row
 constexpr int kPEpiWarps = 16;   // warps 6..21: four per TMEM lane quarter
 constexpr int kPThreads = 32 * (2 + kPBuildWarps + kPEpiWarps);
 constexpr int kPEpiThreads = kPEpiWarps * 32;
-constexpr int kPStages = 4;
-constexpr uint32_t kPRows = 128;  // docs per CTA per tile
 constexpr uint32_t kPMaxN = 256;
 constexpr uint32_t kPKBytes = 128;
-constexpr uint32_t kPAStage = kPRows * kPKBytes;        // 16 KiB
-constexpr uint32_t kPBStage = (kPMaxN / 2) * kPKBytes;  // 16 KiB: this CTA's half of B
-constexpr uint32_t kPSegCap = 256;                      // kept entries per epilogue warp per tile
-constexpr uint32_t kPTmemCols = 512;                    // two accumulators of 256 columns
+constexpr uint32_t kPTmemCols = 512;
 
+// PAIR: CTA pairs, 128 doc rows per CTA, two 256-column accumulators.
+// !PAIR: one CTA per SM, 256 doc rows (two M=128 halves) in one 512-column
+// accumulator; the next tile's MMAs wait for the epilogue's TMEM reads only.
+template <bool PAIR>
+struct PT {
+  static constexpr uint32_t kRows = PAIR ? 128 : 256;  // doc rows per CTA per tile
+  static constexpr int kStages = PAIR ? 4 : 3;
+  static constexpr uint32_t kSegCap = PAIR ? 256 : 192;  // kept entries per epilogue warp per tile
+  static constexpr uint32_t kAStage = kRows * kPKBytes;
+  static constexpr uint32_t kBStage = (PAIR ? kPMaxN / 2 : kPMaxN) * kPKBytes;
+  static constexpr uint32_t kAccBufs = PAIR ? 2 : 1;
+  static constexpr uint32_t kRowsPerThread = kRows / (kPBuildWarps * 32);
+};
+
+template <bool PAIR>
 struct PSmem {
-  uint8_t a[kPStages][kPAStage];
-  uint8_t b[kPStages][kPBStage];
-  uint2 list[kPEpiWarps][kPSegCap];  // (accumulator, q | slot << 8 | row << 16)
+  uint8_t a[PT<PAIR>::kStages][PT<PAIR>::kAStage];
+  uint8_t b[PT<PAIR>::kStages][PT<PAIR>::kBStage];
+  uint2 list[kPEpiWarps][PT<PAIR>::kSegCap];  // (accumulator, q | slot << 8 | row << 16)
   float bias[kPMaxN];
   float invq[kPMaxN];
   uint32_t thr[kPMaxN];
@@ -77,9 +87,9 @@ struct PSmem {
   uint32_t qpop[kPMaxN];  // sign bitmaps: query popcounts
   uint32_t cnt[kPMaxN];
   uint32_t base[kPMaxN];
-  uint64_t full_a[kPStages];
-  uint64_t full_b[kPStages];
-  uint64_t empty[kPStages];
+  uint64_t full_a[PT<PAIR>::kStages];
+  uint64_t full_b[PT<PAIR>::kStages];
+  uint64_t empty[PT<PAIR>::kStages];
   uint64_t acc_full[2];
   uint64_t acc_empty[2];
   uint32_t tmem;
@@ -116,15 +126,18 @@ __device__ __forceinline__ void arrive_remote(uint32_t cluster_addr) {
 // Barriers with arrivals from the other CTA are waited like local ones.
 __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity) { return mbar_wait(bar, parity); }
 
-__device__ __forceinline__ bool aborted(const PSmem& S) {
+template <bool PAIR>
+__device__ __forceinline__ bool aborted(const PSmem<PAIR>& S) {
   return *reinterpret_cast<const volatile uint32_t*>(&S.abort) != 0;
 }
 
-// Sets the abort flag of both CTAs and bit 0 of *err.
-__device__ __forceinline__ void raise_abort(PSmem& S, uint32_t* err) {
+// Sets the abort flag of the CTA (and of its pair) and bit 0 of *err.
+template <bool PAIR>
+__device__ __forceinline__ void raise_abort(PSmem<PAIR>& S, uint32_t* err) {
   atomicExch(&S.abort, 1u);
-  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(peer_addr(smem_u32(&S.abort), cta_rank() ^ 1)), "r"(1u)
-               : "memory");
+  if (PAIR)
+    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(peer_addr(smem_u32(&S.abort), cta_rank() ^ 1)), "r"(1u)
+                 : "memory");
   atomicOr(err, 1u);
 }
 
@@ -160,13 +173,18 @@ struct PairGrid {
   uint32_t n_doc_tiles, q_tiles;
 };
 
-template <int MODE>
+template <int MODE, bool PAIR>
 __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs& a, const PairGrid g) {
+  using T = PT<PAIR>;
+  constexpr int kPStages = T::kStages;
+  constexpr uint32_t kPRows = T::kRows, kPSegCap = T::kSegCap, kBufs = T::kAccBufs;
   extern __shared__ uint8_t smem_raw[];
-  PSmem& S = *reinterpret_cast<PSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  PSmem<PAIR>& S =
+      *reinterpret_cast<PSmem<PAIR>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const uint32_t rank = cta_rank();
-  const uint32_t cluster = blockIdx.x >> 1, n_clusters = gridDim.x >> 1;
+  const uint32_t rank = PAIR ? cta_rank() : 0u;
+  // a "cluster" is a pair of CTAs, or one CTA
+  const uint32_t cluster = PAIR ? blockIdx.x >> 1 : blockIdx.x, n_clusters = PAIR ? gridDim.x >> 1 : gridDim.x;
   const uint64_t total = (uint64_t)g.n_doc_tiles * g.q_tiles;
   const uint32_t nt = a.nt, half = nt / 2;
   const uint32_t n_kb = a.n_kb;
@@ -175,26 +193,36 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
 
   if (t == 32) {
     for (int s = 0; s < kPStages; s++) {
-      mbar_init(&S.full_a[s], 2 * kPBuildWarps);  // builder warps of both CTAs
-      mbar_init(&S.full_b[s], 1);                 // the leader's expect_tx
-      mbar_init(&S.empty[s], 1);                  // the leader's MMA commit
+      mbar_init(&S.full_a[s], (PAIR ? 2 : 1) * kPBuildWarps);  // builder warps of both CTAs
+      mbar_init(&S.full_b[s], 1);                              // the leader's expect_tx
+      mbar_init(&S.empty[s], 1);                               // the leader's MMA commit
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&S.acc_full[b], 1);
-      mbar_init(&S.acc_empty[b], 2 * kPEpiWarps);  // epilogue warps of both CTAs
+      mbar_init(&S.acc_empty[b], (PAIR ? 2 : 1) * kPEpiWarps);  // epilogue warps of both CTAs
     }
     S.abort = 0;
     S.epi_stop = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
-                 "r"(kPTmemCols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    if (PAIR) {
+      asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
+                   "r"(kPTmemCols)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    } else {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
+                   "r"(kPTmemCols)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  cluster_sync_all();  // both CTAs' barriers initialised, TMEM allocated
+  if (PAIR)
+    cluster_sync_all();  // both CTAs' barriers initialised, TMEM allocated
+  else
+    __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = S.tmem;
 
@@ -212,8 +240,11 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
             break;
           }
           if (rank == 0) mbar_expect_tx(&S.full_b[s], nt * kPKBytes);  // both halves
-          tma_load_2d_pair(S.b[s], &b_map, (int)(kb * kPKBytes), (int)(q0 + rank * half),
-                           peer_addr(smem_u32(&S.full_b[s]), 0));
+          if (PAIR)
+            tma_load_2d_pair(S.b[s], &b_map, (int)(kb * kPKBytes), (int)(q0 + rank * half),
+                             peer_addr(smem_u32(&S.full_b[s]), 0));
+          else
+            tma_load_2d(S.b[s], &b_map, (int)(kb * kPKBytes), (int)q0, &S.full_b[s]);
         }
       }
       // the leader waits (bounded) until its last copies, and the peer's, landed
@@ -224,14 +255,14 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
   } else if (warp == 1) {
     // ---- MMA issuer (leader) ------------------------------------------------------
     if (lane == 0 && rank == 0) {
-      // D s32, A/B u8, K-major, N = nt, M = 256 across the pair
-      const uint32_t idesc = (2u << 4) | ((nt >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
+      // D s32, A/B u8, K-major, N = nt; M = 256 across the pair, or two M = 128 halves
+      const uint32_t idesc = (2u << 4) | ((nt >> 3) << 17) | ((uint32_t)((PAIR ? 256 : 128) >> 4) << 24);
       uint64_t it = 0, issued = 0;
       uint32_t tcount = 0;
       bool ok = true;
       for (uint64_t tile = cluster; tile < total && ok; tile += n_clusters, tcount++) {
-        const uint32_t b = tcount & 1;
-        if (tcount >= 2 && !mbar_wait_cluster(&S.acc_empty[b], ((tcount >> 1) - 1) & 1)) ok = false;
+        const uint32_t b = tcount % kBufs;
+        if (tcount >= kBufs && !mbar_wait_cluster(&S.acc_empty[b], (tcount / kBufs - 1) & 1)) ok = false;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + b * 256;
         for (uint32_t kb = 0; kb < n_kb && ok; kb++, it++) {
@@ -242,16 +273,30 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t a0 = smem_u32(S.a[s]), b0 = smem_u32(S.b[s]);
+          if (PAIR) {
 #pragma unroll
-          for (uint32_t j = 0; j < 4; j++)
-            mma_i8_pair(d, sw128_desc(a0 + 32 * j), sw128_desc(b0 + 32 * j), idesc, (kb | j) != 0);
-          commit_pair(smem_u32(&S.empty[s]));
-          commit_pair(peer_addr(smem_u32(&S.empty[s]), 1));
+            for (uint32_t j = 0; j < 4; j++)
+              mma_i8_pair(d, sw128_desc(a0 + 32 * j), sw128_desc(b0 + 32 * j), idesc, (kb | j) != 0);
+            commit_pair(smem_u32(&S.empty[s]));
+            commit_pair(peer_addr(smem_u32(&S.empty[s]), 1));
+          } else {
+#pragma unroll
+            for (uint32_t j = 0; j < 4; j++) {
+              const uint64_t bd = sw128_desc(b0 + 32 * j);
+              mma_i8(d, sw128_desc(a0 + 32 * j), bd, idesc, (kb | j) != 0);
+              mma_i8(d + 256, sw128_desc(a0 + kPRows / 2 * kPKBytes + 32 * j), bd, idesc, (kb | j) != 0);
+            }
+            mma_commit(&S.empty[s]);
+          }
           issued = it + 1;
         }
         if (!ok) break;
-        commit_pair(smem_u32(&S.acc_full[b]));
-        commit_pair(peer_addr(smem_u32(&S.acc_full[b]), 1));
+        if (PAIR) {
+          commit_pair(smem_u32(&S.acc_full[b]));
+          commit_pair(peer_addr(smem_u32(&S.acc_full[b]), 1));
+        } else {
+          mma_commit(&S.acc_full[b]);
+        }
       }
       if (!ok) {
         if (!aborted(S)) raise_abort(S, a.err);
@@ -261,10 +306,11 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
       }
     }
   } else if (warp < 2 + kPBuildWarps) {
-    // ---- A builders (both CTAs): thread r builds doc row r, chunks 0..7 ---------------
+    // ---- A builders: thread r builds doc rows r + 128 i (i < kRowsPerThread), chunks 0..7
+    constexpr uint32_t R = T::kRowsPerThread;
     const uint32_t r = (uint32_t)t - 64;  // 0..127
-    const uint32_t a_row = (r >> 3) * 1024 + (r & 7) * 128;
-    const uint32_t full_a0 = peer_addr(smem_u32(&S.full_a[0]), 0);  // leader's full_a[0]
+    // leader's full_a[0] (a cluster address; the CTA's own barrier when alone)
+    const uint32_t full_a0 = PAIR ? peer_addr(smem_u32(&S.full_a[0]), 0) : 0u;
     uint64_t it = 0;
     bool ok = true;
     // wait for stage s to be free, or stop (warp-uniform)
@@ -281,49 +327,85 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     auto publish = [&](uint32_t s) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
-      if (lane == 0) arrive_remote(full_a0 + 8 * s);
+      if (lane == 0) {
+        if (PAIR)
+          arrive_remote(full_a0 + 8 * s);
+        else
+          mbar_arrive(&S.full_a[s]);
+      }
     };
     for (uint64_t tile = cluster; tile < total && ok; tile += n_clusters) {
       const uint64_t dt = tile / g.q_tiles;
-      const uint64_t pb = (dt * 8 + rank * 4 + (r >> 5)) * a.block_stride;
-      const uint64_t doc = pb * 32 + (r & 31);
+      uint64_t pb[R], doc[R];
+      uint32_t a_row[R];  // row offset in a stage: 8-row atoms of 1024 bytes, 128 bytes a row
+#pragma unroll
+      for (uint32_t i = 0; i < R; i++) {
+        const uint32_t row = r + 128 * i;
+        pb[i] = (dt * 8 + rank * (kPRows / 32) + (row >> 5)) * a.block_stride;
+        doc[i] = pb[i] * 32 + (row & 31);
+        a_row[i] = (row >> 3) * 1024 + (row & 7) * 128;
+      }
       if constexpr (MODE == 1) {
-        const bool row_ok = pb < n_blocks && doc < a.n;
-        const uint64_t* words = reinterpret_cast<const uint64_t*>(a.blocks) + (row_ok ? doc : 0) * (uint64_t)a.qpv;
-        auto word_at = [&](uint32_t wi) -> uint64_t { return (row_ok && wi < a.qpv) ? __ldg(words + wi) : 0ull; };
-        // K-block kb = words 2 kb, 2 kb + 1; two K-blocks of words in flight
-        uint64_t w0 = word_at(0), w1 = word_at(1), w2 = word_at(2), w3 = word_at(3);
+        const uint64_t* words[R];
+        bool row_ok[R];
+        uint64_t w[R][4];  // K-block kb = words 2 kb, 2 kb + 1; two K-blocks of words in flight
+#pragma unroll
+        for (uint32_t i = 0; i < R; i++) {
+          row_ok[i] = pb[i] < n_blocks && doc[i] < a.n;
+          words[i] = reinterpret_cast<const uint64_t*>(a.blocks) + (row_ok[i] ? doc[i] : 0) * (uint64_t)a.qpv;
+#pragma unroll
+          for (uint32_t j = 0; j < 4; j++) w[i][j] = (row_ok[i] && j < a.qpv) ? __ldg(words[i] + j) : 0ull;
+        }
         for (uint32_t kb = 0; kb < n_kb; kb++, it++) {
-          const uint64_t lo = w0, hi = w1;
-          w0 = w2;
-          w1 = w3;
-          w2 = word_at(2 * kb + 4);
-          w3 = word_at(2 * kb + 5);
+          uint64_t lo[R], hi[R];
+#pragma unroll
+          for (uint32_t i = 0; i < R; i++) {
+            lo[i] = w[i][0];
+            hi[i] = w[i][1];
+            w[i][0] = w[i][2];
+            w[i][1] = w[i][3];
+            const uint32_t wi = 2 * kb + 4;
+            w[i][2] = (row_ok[i] && wi < a.qpv) ? __ldg(words[i] + wi) : 0ull;
+            w[i][3] = (row_ok[i] && wi + 1 < a.qpv) ? __ldg(words[i] + wi + 1) : 0ull;
+          }
           const uint32_t s = (uint32_t)(it % kPStages);
           if (!acquire(s)) {
             ok = false;
             break;
           }
-          const uint32_t base = smem_u32(S.a[s]) + a_row;
 #pragma unroll
-          for (uint32_t c = 0; c < 8; c++) {  // 16 coordinates per 16-byte chunk
-            const uint32_t h = (uint32_t)((c < 4 ? lo : hi) >> (16 * (c & 3)));
-            uint32_t o[4];
+          for (uint32_t i = 0; i < R; i++) {
+            const uint32_t base = smem_u32(S.a[s]) + a_row[i], rr = (r + 128 * i) & 7;
 #pragma unroll
-            for (uint32_t i = 0; i < 4; i++)  // 4 bits -> 4 bytes (the shifted copies never overlap)
-              o[i] = (((h >> (4 * i)) & 15u) * 0x00204081u) & 0x01010101u;
-            st_shared_v4(base + ((c ^ (r & 7)) << 4), o[0], o[1], o[2], o[3]);
+            for (uint32_t c = 0; c < 8; c++) {  // 16 coordinates per 16-byte chunk
+              const uint32_t h = (uint32_t)((c < 4 ? lo[i] : hi[i]) >> (16 * (c & 3)));
+              uint32_t o[4];
+#pragma unroll
+              for (uint32_t q = 0; q < 4; q++)  // 4 bits -> 4 bytes (the shifted copies never overlap)
+                o[q] = (((h >> (4 * q)) & 15u) * 0x00204081u) & 0x01010101u;
+              st_shared_v4(base + ((c ^ rr) << 4), o[0], o[1], o[2], o[3]);
+            }
           }
           publish(s);
         }
       } else {
-        const bool row_valid = pb < n_blocks;
-        const uint8_t* row_codes = a.blocks + pb * (uint64_t)a.pairs_pad * 16 + (uint64_t)(r & 31) * 16;
+        const uint8_t* row_codes[R];
+        bool row_valid[R];
+        uint4 next[R];
+#pragma unroll
+        for (uint32_t i = 0; i < R; i++) {
+          row_valid[i] = pb[i] < n_blocks;
+          row_codes[i] = a.blocks + pb[i] * (uint64_t)a.pairs_pad * 16 + (uint64_t)((r + 128 * i) & 31) * 16;
+          next[i] = row_valid[i] ? load_codes(row_codes[i]) : make_uint4(0, 0, 0, 0);
+        }
         const uint32_t n_groups = n_kb / 4;  // one 16-byte code load covers 4 K-blocks
-        uint4 next = row_valid ? load_codes(row_codes) : make_uint4(0, 0, 0, 0);
         for (uint32_t gi = 0; gi < n_groups && ok; gi++) {
-          const uint4 chunk = next;
-          if (row_valid && gi + 1 < n_groups) next = load_codes(row_codes + (uint64_t)(gi + 1) * 512);
+          uint4 chunk[R];
+#pragma unroll
+          for (uint32_t i = 0; i < R; i++) {
+            chunk[i] = next[i];
+            if (row_valid[i] && gi + 1 < n_groups) next[i] = load_codes(row_codes[i] + (uint64_t)(gi + 1) * 512);
+          }
 #pragma unroll
           for (uint32_t j = 0; j < 4; j++) {
             const uint32_t s = (uint32_t)(it % kPStages);
@@ -331,12 +413,15 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
               ok = false;
               break;
             }
-            const uint32_t w = j == 0 ? chunk.x : j == 1 ? chunk.y : j == 2 ? chunk.z : chunk.w;
-            const uint32_t base = smem_u32(S.a[s]) + a_row;
 #pragma unroll
-            for (uint32_t c = 0; c < 8; c++) {
-              const uint32_t sh = c == 0 ? (w << 3) & 0x78u : (w >> (4 * c - 3)) & 0x78u;  // 8 * nibble c
-              st_shared_v4(base + ((c ^ (r & 7)) << 4), shl1(sh), shl1(sh - 32), shl1(sh - 64), shl1(sh - 96));
+            for (uint32_t i = 0; i < R; i++) {
+              const uint32_t wv = j == 0 ? chunk[i].x : j == 1 ? chunk[i].y : j == 2 ? chunk[i].z : chunk[i].w;
+              const uint32_t base = smem_u32(S.a[s]) + a_row[i], rr = (r + 128 * i) & 7;
+#pragma unroll
+              for (uint32_t c = 0; c < 8; c++) {
+                const uint32_t sh = c == 0 ? (wv << 3) & 0x78u : (wv >> (4 * c - 3)) & 0x78u;  // 8 * nibble c
+                st_shared_v4(base + ((c ^ rr) << 4), shl1(sh), shl1(sh - 32), shl1(sh - 64), shl1(sh - 96));
+              }
             }
             publish(s);
             it++;
@@ -348,9 +433,15 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     // ---- epilogue (both CTAs) -------------------------------------------------------
     const uint32_t e = (uint32_t)warp - 2 - kPBuildWarps;  // 0..15
     const uint32_t et = (uint32_t)t - 32 * (2 + kPBuildWarps);
-    const uint32_t lq = (uint32_t)warp & 3, cq = e >> 2;  // lane quarter, column quarter
-    const uint32_t row = lq * 32 + lane;
-    const uint32_t acc_empty0 = peer_addr(smem_u32(&S.acc_empty[0]), 0);
+    // TMEM lane quarter (hardware rule: warp % 4); PAIR: column quarter e / 4 of
+    // the CTA's 128 rows; !PAIR: accumulator half (rows 0..127 | 128..255) and
+    // column half
+    const uint32_t lq = (uint32_t)warp & 3;
+    const uint32_t h = PAIR ? 0u : (e >> 2) & 1;
+    const uint32_t col0 = PAIR ? (e >> 2) * 64 : (e >> 3) * 128;
+    constexpr uint32_t kChunks = PAIR ? 2 : 4;  // 32-column chunks per warp
+    const uint32_t row = h * 128 + lq * 32 + lane;
+    const uint32_t acc_empty0 = PAIR ? peer_addr(smem_u32(&S.acc_empty[0]), 0) : 0u;
     uint2* list = S.list[e];
     uint32_t lt;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
@@ -358,7 +449,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     for (uint64_t tile = cluster; tile < total; tile += n_clusters, tcount++) {
       const uint64_t dt = tile / g.q_tiles, q0 = (tile % g.q_tiles) * nt;
       const uint32_t nqt = (uint32_t)((a.nq - q0) < nt ? (a.nq - q0) : nt);
-      const uint32_t b = tcount & 1;
+      const uint32_t b = tcount % kBufs;
       // per-query parameters of this tile (the previous tile's slot passes are done)
       epi_sync();
       if (et == 0) {
@@ -400,7 +491,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
         if (S.amin[i] == kExactCompare) atomicOr(&S.any_exact, 1u);
       // wait for the accumulator; one verdict for all epilogue warps
       bool ready = false;
-      if (lane == 0) ready = !aborted(S) && mbar_wait_cluster(&S.acc_full[b], (tcount >> 1) & 1);
+      if (lane == 0) ready = !aborted(S) && mbar_wait_cluster(&S.acc_full[b], (tcount / kBufs) & 1);
       ready = __shfl_sync(0xFFFFFFFFu, ready, 0);
       if (!ready && lane == 0) {
         if (!aborted(S)) raise_abort(S, a.err);
@@ -409,16 +500,16 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
       epi_sync();
       if (*reinterpret_cast<volatile uint32_t*>(&S.epi_stop)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint64_t pb = (dt * 8 + rank * 4 + lq) * a.block_stride;
+      const uint64_t pb = (dt * 8 + rank * (kPRows / 32) + (row >> 5)) * a.block_stride;
       const uint64_t doc = pb * 32 + lane;
       const uint64_t u = dt * 256 + rank * kPRows + row;
       const bool valid = pb < n_blocks && doc < a.n;
       const uint32_t dpop = (MODE == 1 && a.key_kind == 2) ? row_popcount(a, doc, valid) : 0u;
-      const uint32_t taddr = tmem + ((lq * 32) << 16) + b * 256;
+      const uint32_t taddr = tmem + ((lq * 32) << 16) + (b + h) * 256;
       const bool any_exact = S.any_exact != 0;
       uint32_t wcount = 0;
-      for (uint32_t c = 0; c < 2; c++) {
-        const uint32_t cb = cq * 64 + c * 32;
+      for (uint32_t c = 0; c < kChunks; c++) {
+        const uint32_t cb = col0 + c * 32;
         if (cb >= nt) break;  // warp-uniform
         uint32_t v[32];
         __syncwarp();
@@ -479,7 +570,12 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
       // the accumulator is in registers / the list: release it to the MMA
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
-      if (lane == 0) arrive_remote(acc_empty0 + 8 * b);
+      if (lane == 0) {
+        if (PAIR)
+          arrive_remote(acc_empty0 + 8 * b);
+        else
+          mbar_arrive(&S.acc_empty[b]);
+      }
       if (!dense) {
         // slots within each query's share of the tile, one global atomic per
         // query per tile, then each warp writes its segment
@@ -505,7 +601,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           if (pos < a.cap) {
             a.f_keys[(q0 + q) * a.cap + pos] =
                 MODE == 0 ? desc_key(tc_score(en.x, S.bias[q], S.invq[q], a.inv_norm)) : bm_key_q(a, S.qpop[q], en.x);
-            const uint64_t rpb = (dt * 8 + rank * 4 + (rw >> 5)) * a.block_stride;
+            const uint64_t rpb = (dt * 8 + rank * (kPRows / 32) + (rw >> 5)) * a.block_stride;
             a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw & 31));
           }
         }
@@ -514,20 +610,34 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  cluster_sync_all();  // neither CTA frees the pair's tensor memory while the other uses it
+  if (PAIR) cluster_sync_all();  // neither CTA frees the pair's tensor memory while the other uses it
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (warp == 1)
-    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kPTmemCols) : "memory");
+  if (warp == 1) {
+    if (PAIR)
+      asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kPTmemCols) : "memory");
+    else
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kPTmemCols) : "memory");
+  }
 }
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     fastscan_pair_kernel(const __grid_constant__ CUtensorMap b_map, const TcArgs a, const PairGrid g) {
-  pair_body<0>(b_map, a, g);
+  pair_body<0, true>(b_map, a, g);
 }
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     bitmap_pair_kernel(const __grid_constant__ CUtensorMap b_map, const TcArgs a, const PairGrid g) {
-  pair_body<1>(b_map, a, g);
+  pair_body<1, true>(b_map, a, g);
+}
+
+__global__ void __launch_bounds__(kPThreads, 1)
+    fastscan_persist_kernel(const __grid_constant__ CUtensorMap b_map, const TcArgs a, const PairGrid g) {
+  pair_body<0, false>(b_map, a, g);
+}
+
+__global__ void __launch_bounds__(kPThreads, 1)
+    bitmap_persist_kernel(const __grid_constant__ CUtensorMap b_map, const TcArgs a, const PairGrid g) {
+  pair_body<1, false>(b_map, a, g);
 }
 
 // clusters of two that can be resident at once (each CTA takes a whole SM)
@@ -556,18 +666,24 @@ uint32_t resident_pairs(const void* kernel, size_t smem) {
 
 }  // namespace
 
-// Default: the bitmap family on pairs (1-CTA form epilogue-bound: measured
-// 22 % faster on pairs), FastScan on one CTA per tile (both forms are bound by
-// the MMA rate there, and the 1-CTA form keeps the tensor pipe busier).
-bool tc_pair_enabled(int mode) {
+// Which tensor-core scan form a launch uses: OVB_TC_FORM=tile|persist|pair
+// forces one (OVB_TC_PAIR=0/1 is tile/pair).  Default: the bitmap family on
+// CTA pairs (the one-CTA form is epilogue-bound there: 22 % slower);
+// FastScan on the persistent one-CTA form, both being bound by the MMA rate.
+TcForm tc_form(int mode) {
+  const char* f = getenv("OVB_TC_FORM");
+  if (f && f[0]) return f[0] == 't' ? TcForm::kTile : f[1] == 'e' ? TcForm::kPersist : TcForm::kPair;
   const char* e = getenv("OVB_TC_PAIR");
-  if (e && e[0] == '0') return false;
-  if (e && e[0] == '1') return true;
-  return mode == 1;
+  if (e && e[0] == '0') return TcForm::kTile;
+  if (e && e[0] == '1') return TcForm::kPair;
+  return mode == 1 ? TcForm::kPair : TcForm::kPersist;
 }
 
+// kept entries one epilogue warp of the persistent one-CTA form may hold per tile
+uint32_t tc_persist_seg_cap() { return PT<false>::kSegCap; }
+
 template <int MODE>
-void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream) {
+void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool pair) {
   if (!a.n || !a.nq) return;
   const char* what = MODE == 0 ? "FastScan tensor-core scan" : "bitmap tensor-core scan";
   const uint64_t k_bytes = (uint64_t)a.n_kb * kPKBytes;
@@ -576,7 +692,7 @@ void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream) {
   CUtensorMap map;
   cuuint64_t gdim[2] = {(cuuint64_t)k_bytes, (cuuint64_t)a.nq};
   cuuint64_t gstride[1] = {(cuuint64_t)k_bytes};
-  cuuint32_t box[2] = {(cuuint32_t)kPKBytes, (cuuint32_t)(a.nt / 2)};
+  cuuint32_t box[2] = {(cuuint32_t)kPKBytes, (cuuint32_t)(pair ? a.nt / 2 : a.nt)};
   cuuint32_t estride[2] = {1, 1};
   CUresult rc = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)b_rows, gdim, gstride, box, estride,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -586,9 +702,6 @@ void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream) {
   if (MODE == 1 && (64ull * a.qpv >= (1ull << 24) || 2ull * a.n_kb < a.qpv))
     throw std::invalid_argument(std::string(what) + ": row too long");
   if (!a.keys && a.block_stride != 1) throw std::invalid_argument(std::string(what) + ": filter needs stride 1");
-  auto kernel = MODE == 0 ? fastscan_pair_kernel : bitmap_pair_kernel;
-  const size_t smem = sizeof(PSmem) + 1024;
-  OVB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const uint64_t n_blocks = (a.n + 31) / 32;
   const uint64_t logical_blocks = (n_blocks + a.block_stride - 1) / a.block_stride;
   PairGrid g;
@@ -599,13 +712,28 @@ void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream) {
   g.n_doc_tiles = (uint32_t)doc_tiles;
   g.q_tiles = (uint32_t)q_tiles;
   const uint64_t total = doc_tiles * q_tiles;
-  uint64_t clusters = resident_pairs((const void*)kernel, smem);
-  if (clusters > total) clusters = total;
-  kernel<<<(unsigned)(2 * clusters), kPThreads, smem, stream>>>(map, a, g);
+  if (pair) {
+    auto kernel = MODE == 0 ? fastscan_pair_kernel : bitmap_pair_kernel;
+    const size_t smem = sizeof(PSmem<true>) + 1024;
+    OVB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    uint64_t clusters = resident_pairs((const void*)kernel, smem);
+    if (clusters > total) clusters = total;
+    kernel<<<(unsigned)(2 * clusters), kPThreads, smem, stream>>>(map, a, g);
+  } else {
+    auto kernel = MODE == 0 ? fastscan_persist_kernel : bitmap_persist_kernel;
+    const size_t smem = sizeof(PSmem<false>) + 1024;
+    OVB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 0;
+    OVB_CUDA(cudaGetDevice(&dev));
+    OVB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    uint64_t ctas = (uint64_t)sms;  // one CTA per SM (its shared memory and TMEM fill the SM)
+    if (ctas > total) ctas = total;
+    kernel<<<(unsigned)ctas, kPThreads, smem, stream>>>(map, a, g);
+  }
   launched();
 }
 
-template void launch_tc_pair<0>(TcArgs, const uint8_t*, cudaStream_t);
-template void launch_tc_pair<1>(TcArgs, const uint8_t*, cudaStream_t);
+template void launch_tc_pair<0>(TcArgs, const uint8_t*, cudaStream_t, bool);
+template void launch_tc_pair<1>(TcArgs, const uint8_t*, cudaStream_t, bool);
 
 }  // namespace ovb

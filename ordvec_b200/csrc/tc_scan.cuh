@@ -42,6 +42,7 @@ struct TcArgs {
   uint32_t* f_keys;
   uint32_t* f_ids;
   uint32_t* err;
+  uint64_t expect_kept;  // filter: expected kept docs per query (0 = unknown)
 };
 
 // shl.b32 clamps shift amounts >= 32 to 32 (result 0); a "negative" amount
@@ -150,11 +151,13 @@ __device__ __forceinline__ uint4 load_codes(const uint8_t* p) {
 // B = query bits as 0/1 bytes, acc = overlap, key = n_top - overlap).
 }  // namespace tcs
 
-// The persistent CTA-pair form (scan_tc_pair.cu) of the same scans.  MODE 0
-// FastScan, 1 bitmap; b_rows = the query operand.  tc_pair_enabled(mode): the
-// default choice for the mode, OVB_TC_PAIR=0/1 forces.
-bool tc_pair_enabled(int mode);
+// Forms of the tensor-core scans: one CTA per 256-doc tile (scan_fastscan_tc.cu),
+// and the persistent forms of scan_tc_pair.cu: one CTA per SM, or CTA pairs.
+enum class TcForm { kTile, kPersist, kPair };
+TcForm tc_form(int mode);  // MODE 0 FastScan, 1 bitmap
+uint32_t tc_persist_seg_cap();
+// b_rows = the query operand; pair: CTA pairs, else one CTA per SM
 template <int MODE>
-void launch_tc_pair(tcs::TcArgs a, const uint8_t* b_rows, cudaStream_t stream);
+void launch_tc_pair(tcs::TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool pair);
 
 }  // namespace ovb

@@ -645,8 +645,9 @@ def test_bitmap_tensor_core_top_m_is_exact(orc, monkeypatch, dim, n_top, n, nq, 
 
 @pytest.mark.parametrize("kind", ["fastscan", "bitmap", "multibucket", "sign"])
 def test_cta_pair_scan_matches_single_cta(monkeypatch, kind):
-    """The persistent CTA-pair tensor-core kernel (cta_group::2, double-buffered
-    accumulators) and the one-CTA-per-tile kernel give identical results, on
+    """The three forms of the tensor-core scans -- one CTA per tile, the
+    persistent one-CTA-per-SM kernel, and the persistent CTA-pair kernel
+    (cta_group::2, double-buffered accumulators) -- give identical results, on
     the sampled threshold pass, the filter and the dense key matrix, with a
     partial last query tile and a partial last doc tile."""
     n, nq = 70_001, 300
@@ -673,12 +674,12 @@ def test_cta_pair_scan_matches_single_cta(monkeypatch, kind):
     monkeypatch.setenv("OVB_FASTSCAN_TC", "1")
     monkeypatch.setenv("OVB_BITMAP_TC", "1")
     out = {}
-    for pair in ("0", "1"):
+    for form in ("tile", "persist", "pair"):
         for filt in ("0", "1"):
-            monkeypatch.setenv("OVB_TC_PAIR", pair)
+            monkeypatch.setenv("OVB_TC_FORM", form)
             monkeypatch.setenv("OVB_FASTSCAN_FILTER", filt)
-            out[(pair, filt)] = run()
-    base = out[("0", "0")]
+            out[(form, filt)] = run()
+    base = out[("tile", "0")]
     for key, got in out.items():
         if kind in ("multibucket", "sign"):
             assert np.array_equal(got, base), key
