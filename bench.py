@@ -39,9 +39,9 @@ METRIC = "QPS & scan HBM GB/s vs peak, batched vs plain GPU @ identical top-10; 
 N_DOCS, DIM, NQ, K, M = 171_332, 1024, 1000, 10, 1000
 SEED = 0x0DD5EED2
 STAGES = ["prep", "threshold", "scan", "select", "rerank", "final_select"]
-# DRAM traffic of one filter launch of fastscan_tc_kernel at this workload, from an ncu capture
-# (53,136,896 B read + 8,834,304 B written): the codes and LUTs cross HBM about once.
-TC_FILTER_DRAM_BYTES = 53_136_896 + 8_834_304
+# DRAM traffic of one filter launch of fastscan_persist_kernel at this workload, from an ncu capture
+# (52,310,016 B read + 2,875,392 B written): the codes and LUTs cross HBM about once.
+TC_FILTER_DRAM_BYTES = 52_310_016 + 2_875_392
 WORKLOAD = (f"fastscan_two_stage: RankQuantFastscan top-{M} -> RankQuant b=2 asymmetric rerank top-{K}; "
             f"N={N_DOCS} dim={DIM}; {NQ} queries per step")
 
@@ -696,7 +696,7 @@ def main():
                 "frac": achieved / peak, "traffic": TC_FILTER_DRAM_BYTES,
                 "traffic_unit": "DRAM bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                 "algorithmic_hbm_bytes_per_launch": code_bytes + nq * pairs_pad * 16,
-                "kernel": "fastscan_tc_kernel (filter epilogue)",
+                "kernel": "fastscan_persist_kernel (filter epilogue)",
                 "queries_per_launch": nq, "algorithmic_ops_per_launch": ops, "launch_ms": ms,
                 "peak_source": f"2 x {peak_kind} bf16 dense TFLOP/s (burst)"}
 
