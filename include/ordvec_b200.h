@@ -144,25 +144,30 @@ ordvec_status_t ordvec_index_search(const ordvec_index_t *index,
 #define OVB_INDEX_KIND_SIGN_BITMAP 3  /* src/sign_bitmap.rs SignBitmap */
 #define OVB_INDEX_KIND_FASTSCAN 4     /* src/fastscan.rs RankQuantFastscan */
 #define OVB_INDEX_KIND_MULTIBUCKET 5  /* src/multi_bucket.rs MultiBucketBitmap */
+#define OVB_INDEX_KIND_RANK 6         /* src/rank.rs Rank (u16 rank per coordinate) */
 
 /* Empty device-resident indices; parameters validated as the reference's
  * constructors do (src/quant.rs:375-491, src/sign_bitmap.rs:113-165,
- * src/bitmap.rs:71-125, src/fastscan.rs:568-589, src/multi_bucket.rs:70-93). */
+ * src/bitmap.rs:71-125, src/fastscan.rs:568-589, src/multi_bucket.rs:70-93,
+ * src/rank.rs:316-324). */
 ordvec_status_t ovb_rankquant_new(uint32_t dim, uint32_t bits, ordvec_index_t **out);
 ordvec_status_t ovb_sign_bitmap_new(uint32_t dim, ordvec_index_t **out);
 ordvec_status_t ovb_bitmap_new(uint32_t dim, uint32_t n_top, ordvec_index_t **out);
 ordvec_status_t ovb_fastscan_new(uint32_t dim, ordvec_index_t **out);
 ordvec_status_t ovb_multibucket_new(uint32_t dim, uint32_t bits, ordvec_index_t **out);
+/* Rank: one u16 rank per coordinate, 2 * dim bytes per document; 2 <= dim <= 65535
+ * (adds and searches run the device rank transform: dim <= 16384). */
+ordvec_status_t ovb_rank_new(uint32_t dim, ordvec_index_t **out);
 
 /* `add` (RankQuant::add src/quant.rs:587, SignBitmap::add src/sign_bitmap.rs:180,
  * Bitmap::add src/bitmap.rs:140, RankQuantFastscan::add src/fastscan.rs:597,
- * MultiBucketBitmap::add src/multi_bucket.rs:95): n row-major f32 vectors,
+ * MultiBucketBitmap::add src/multi_bucket.rs:95, Rank::add src/rank.rs:335): n row-major f32 vectors,
  * host or device memory; encoded on the GPU.  Non-finite input is
  * rejected with BAD_ARGUMENT (the reference panics). */
 ordvec_status_t ovb_index_add(ordvec_index_t *index, const float *vectors, uint64_t n);
 ordvec_status_t ovb_index_add_device(ordvec_index_t *index, const float *d_vectors, uint64_t n);
-/* Persisted-format loaders for all four scan formats (.ovrq .ovbm .ovsb
- * .ovfs, src/rank_io.rs), with the reference loader's validation. */
+/* Persisted-format loaders for the scan formats and Rank (.ovrq .ovbm .ovsb
+ * .ovfs .ovr, src/rank_io.rs), with the reference loader's validation. */
 ordvec_status_t ovb_index_load_any(const char *path, uint64_t flags, ordvec_index_t **out);
 ordvec_status_t ovb_index_write(const ordvec_index_t *index, const char *path);
 /* Codes in the reference's persisted payload layout (the bytes after the
@@ -186,6 +191,21 @@ ordvec_status_t ovb_rankquant_search(const ordvec_index_t *rq, const float *quer
 ordvec_status_t ovb_rankquant_search_split(const ordvec_index_t *rq, const float *queries,
                                            uint64_t nq, uint64_t k, uint32_t exact,
                                            float *scores, int64_t *ids);
+/* RankQuant::search, symmetric (src/quant.rs:629-695): the query is
+ * rank-transformed and bucketed like a document; score = sum_d
+ * centre(q_bucket) * centre(d_bucket) / norm^2, the reference's values bit for
+ * bit (the integer-valued sum is exact in f32 for b <= 4). */
+ordvec_status_t ovb_rankquant_search_symmetric(const ordvec_index_t *rq, const float *queries,
+                                               uint64_t nq, uint64_t k, float *scores, int64_t *ids);
+/* Rank::search (src/rank.rs:364-419): Spearman correlation of the query's
+ * ranks with each document's, exact integer sum, then * 0.25 / norm^2 in f32. */
+ordvec_status_t ovb_rank_search(const ordvec_index_t *rank, const float *queries, uint64_t nq,
+                                uint64_t k, float *scores, int64_t *ids);
+/* Rank::search_asymmetric (src/rank.rs:420-482): L2-normalised f32 query
+ * against the stored ranks, (sum_d q[d] rank[d] - mean sum_d q[d]) / norm with
+ * the reference's sequential f32 sums. */
+ordvec_status_t ovb_rank_search_asymmetric(const ordvec_index_t *rank, const float *queries,
+                                           uint64_t nq, uint64_t k, float *scores, int64_t *ids);
 /* Mixed batch (no counterpart in the reference): query i is searched in full
  * in indices[index_of_query[i]] (RankQuant indices of one dim, e.g. one
  * corpus at bits 1, 2 and 4) for its own k_of_query[i] <= k_max, all in one

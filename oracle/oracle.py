@@ -48,6 +48,10 @@ _SIGS = {
     "orc_topk_finalize": (None, [C.c_void_p, f32p, i64p, U64]),
     "orc_topk_free": (None, [C.c_void_p]),
     "orc_rq_search_asym": (U64, [u8p, U64, U32, U32, f32p, U64, U64, f32p, i64p]),
+    "orc_rq_search_sym": (U64, [u8p, U64, U32, U32, f32p, U64, U64, f32p, i64p]),
+    "orc_rank_encode": (None, [f32p, U64, U32, u16p]),
+    "orc_rank_search_sym": (U64, [u16p, U64, U32, f32p, U64, U64, f32p, i64p]),
+    "orc_rank_search_asym": (U64, [u16p, U64, U32, f32p, U64, U64, f32p, i64p]),
     "orc_rq_scores_f64": (None, [u8p, U64, U32, U32, f32p, f64p]),
     "orc_rq_scores_f64_subset": (None, [u8p, U32, U32, f32p, u32p, U64, f64p]),
     "orc_rq_subset": (U64, [u8p, U64, U32, U32, f32p, u32p, U64, U64, f32p, i64p]),
@@ -230,6 +234,37 @@ def rq_search_asym(packed, n, dim, bits, queries, k):
     i = np.empty(nq * ke, np.int64)
     if ke:
         lib().orc_rq_search_asym(np.ascontiguousarray(packed, np.uint8), n, dim, bits, q, nq, k, s, i)
+    return s.reshape(nq, ke), i.reshape(nq, ke)
+
+
+def rq_search_sym(packed, n, dim, bits, queries, k):
+    """RankQuant::search (symmetric): (scores, ids) nq x min(k, n)."""
+    q, nq = _rows(queries, dim)
+    ke = min(k, n)
+    s = np.empty(nq * ke, np.float32)
+    i = np.empty(nq * ke, np.int64)
+    if ke:
+        lib().orc_rq_search_sym(np.ascontiguousarray(packed, np.uint8), n, dim, bits, q, nq, k, s, i)
+    return s.reshape(nq, ke), i.reshape(nq, ke)
+
+
+def rank_encode(vecs, dim):
+    """Rank index rows: u16 rank per coordinate."""
+    v, n = _rows(vecs, dim)
+    out = np.empty(max(n * dim, 1), np.uint16)
+    lib().orc_rank_encode(v, n, dim, out)
+    return out[: n * dim]
+
+
+def rank_search(ranks, n, dim, queries, k, asymmetric=False):
+    """Rank::search / Rank::search_asymmetric: (scores, ids) nq x min(k, n)."""
+    q, nq = _rows(queries, dim)
+    ke = min(k, n)
+    s = np.empty(nq * ke, np.float32)
+    i = np.empty(nq * ke, np.int64)
+    if ke:
+        fn = lib().orc_rank_search_asym if asymmetric else lib().orc_rank_search_sym
+        fn(np.ascontiguousarray(ranks, np.uint16), n, dim, q, nq, k, s, i)
     return s.reshape(nq, ke), i.reshape(nq, ke)
 
 

@@ -429,6 +429,103 @@ uint64_t orc_rq_search_asym(const uint8_t *packed, uint64_t n, uint32_t dim, uin
     return ke;
 }
 
+/* RankQuant::search, symmetric (src/quant.rs:629-695): the query is
+ * rank-transformed and bucketed like a document; LUT[d][b] =
+ * bucket_centre(q_bucket[d]) * bucket_centre(b); the per-document sum is the
+ * scan_b{1,2,4}_to_topk sequential f32 LUT sum, times 1 / (norm * norm). */
+uint64_t orc_rq_search_sym(const uint8_t *packed, uint64_t n, uint32_t dim, uint32_t bits,
+                           const float *queries, uint64_t nq, uint64_t k, float *scores, int64_t *ids) {
+    uint64_t ke = k < n ? k : n;
+    if (ke == 0) return 0;
+    float norm = orc_rankquant_norm(dim, bits);
+    float inv_norm_sq = 1.0f / (norm * norm);
+    uint32_t bpv = dim * bits / 8, nb = 1u << bits;
+    uint16_t *qr = (uint16_t *)malloc(sizeof(uint16_t) * dim);
+    float *lut = (float *)malloc(sizeof(float) * (size_t)dim * nb);
+    for (uint64_t qi = 0; qi < nq; qi++) {
+        orc_rank_transform(queries + qi * dim, dim, qr);
+        for (uint32_t d = 0; d < dim; d++) {
+            float qc = orc_bucket_centre(orc_rank_to_bucket(qr[d], dim, bits), bits);
+            for (uint32_t b = 0; b < nb; b++) lut[d * nb + b] = qc * orc_bucket_centre(b, bits);
+        }
+        orc_topk *t = orc_topk_new(ke, NULL, 0);
+        for (uint64_t di = 0; di < n; di++)
+            orc_topk_insert(t, lut_doc_score(packed + di * bpv, dim, bits, lut) * inv_norm_sq, di);
+        orc_topk_finalize(t, scores + qi * ke, ids + qi * ke, ke);
+        orc_topk_free(t);
+    }
+    free(lut);
+    free(qr);
+    return ke;
+}
+
+/* Rank (src/rank.rs:283-482): one u16 rank per coordinate. */
+void orc_rank_encode(const float *vecs, uint64_t n, uint32_t dim, uint16_t *out) {
+    for (uint64_t i = 0; i < n; i++) orc_rank_transform(vecs + i * dim, dim, out + i * dim);
+}
+
+/* rank_norm (src/rank.rs:249-252): f64 closed form, narrowed to f32. */
+float orc_rank_norm(uint32_t d) {
+    double x = (double)d;
+    return (float)sqrt(x * (x * x - 1.0) / 12.0);
+}
+
+/* Rank::search (src/rank.rs:364-419): Spearman in exact integers,
+ * acc = sum (2 q_r - (D - 1)) (2 d_r - (D - 1)), score = (acc as f32) * 0.25
+ * * (1 / (norm * norm)), left to right in f32. */
+uint64_t orc_rank_search_sym(const uint16_t *ranks, uint64_t n, uint32_t dim, const float *queries,
+                             uint64_t nq, uint64_t k, float *scores, int64_t *ids) {
+    uint64_t ke = k < n ? k : n;
+    if (ke == 0) return 0;
+    float norm = orc_rank_norm(dim);
+    float inv_norm_sq = 1.0f / (norm * norm);
+    int32_t mean_2x = (int32_t)dim - 1;
+    uint16_t *qr = (uint16_t *)malloc(sizeof(uint16_t) * dim);
+    for (uint64_t qi = 0; qi < nq; qi++) {
+        orc_rank_transform(queries + qi * dim, dim, qr);
+        orc_topk *t = orc_topk_new(ke, NULL, 0);
+        for (uint64_t di = 0; di < n; di++) {
+            const uint16_t *doc = ranks + di * dim;
+            int64_t acc = 0;
+            for (uint32_t d = 0; d < dim; d++)
+                acc += (int64_t)(2 * (int32_t)qr[d] - mean_2x) * (int64_t)(2 * (int32_t)doc[d] - mean_2x);
+            orc_topk_insert(t, (float)acc * 0.25f * inv_norm_sq, di);
+        }
+        orc_topk_finalize(t, scores + qi * ke, ids + qi * ke, ke);
+        orc_topk_free(t);
+    }
+    free(qr);
+    return ke;
+}
+
+/* Rank::search_asymmetric (src/rank.rs:420-482): q_unit = l2_normalise(q),
+ * q_sum = sequential f32 sum, acc = sequential f32 sum of q_unit[d] * rank,
+ * score = (acc - mean * q_sum) * (1 / norm), mean = (D - 1) / 2 in f32. */
+uint64_t orc_rank_search_asym(const uint16_t *ranks, uint64_t n, uint32_t dim, const float *queries,
+                              uint64_t nq, uint64_t k, float *scores, int64_t *ids) {
+    uint64_t ke = k < n ? k : n;
+    if (ke == 0) return 0;
+    float inv_norm = 1.0f / orc_rank_norm(dim);
+    float mean = ((float)dim - 1.0f) / 2.0f;
+    float *qu = (float *)malloc(sizeof(float) * dim);
+    for (uint64_t qi = 0; qi < nq; qi++) {
+        orc_l2_normalise(queries + qi * dim, dim, qu);
+        float q_sum = -0.0f;
+        for (uint32_t d = 0; d < dim; d++) q_sum += qu[d];
+        orc_topk *t = orc_topk_new(ke, NULL, 0);
+        for (uint64_t di = 0; di < n; di++) {
+            const uint16_t *doc = ranks + di * dim;
+            float acc = 0.0f;
+            for (uint32_t d = 0; d < dim; d++) acc += qu[d] * (float)doc[d];
+            orc_topk_insert(t, (acc - mean * q_sum) * inv_norm, di);
+        }
+        orc_topk_finalize(t, scores + qi * ke, ids + qi * ke, ke);
+        orc_topk_free(t);
+    }
+    free(qu);
+    return ke;
+}
+
 /* The FP64 reference score of the asymmetric definition
  * score = sum_j q_unit[j] * bucket_centre(code_j) * inv_norm
  * (src/quant.rs:697-704), with q_unit and inv_norm exactly as the

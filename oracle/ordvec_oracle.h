@@ -57,6 +57,16 @@ void orc_topk_insert(orc_topk *t, float score, uint64_t idx);
 void orc_topk_finalize(const orc_topk *t, float *scores, int64_t *indices, uint64_t len);
 void orc_topk_free(orc_topk *t);
 
+/* ---- RankQuant symmetric search; Rank (u16) index ---- */
+uint64_t orc_rq_search_sym(const uint8_t *packed, uint64_t n, uint32_t dim, uint32_t bits,
+                           const float *queries, uint64_t nq, uint64_t k, float *scores, int64_t *ids);
+void orc_rank_encode(const float *vecs, uint64_t n, uint32_t dim, uint16_t *out);
+float orc_rank_norm(uint32_t d);
+uint64_t orc_rank_search_sym(const uint16_t *ranks, uint64_t n, uint32_t dim, const float *queries,
+                             uint64_t nq, uint64_t k, float *scores, int64_t *ids);
+uint64_t orc_rank_search_asym(const uint16_t *ranks, uint64_t n, uint32_t dim, const float *queries,
+                              uint64_t nq, uint64_t k, float *scores, int64_t *ids);
+
 /* ---- RankQuant asymmetric search (scalar LUT tier) ---- */
 uint64_t orc_rq_search_asym(const uint8_t *packed, uint64_t n, uint32_t dim, uint32_t bits,
                             const float *queries, uint64_t nq, uint64_t k, float *scores,

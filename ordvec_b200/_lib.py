@@ -19,7 +19,7 @@ STATUS_NAMES = {
     10: "BUFFER_TOO_SMALL", 11: "UNSUPPORTED_OPERATION", 12: "PANIC", 13: "INTERNAL",
 }
 
-KIND_RANK_QUANT, KIND_BITMAP, KIND_SIGN_BITMAP, KIND_FASTSCAN, KIND_MULTIBUCKET = 1, 2, 3, 4, 5
+KIND_RANK_QUANT, KIND_BITMAP, KIND_SIGN_BITMAP, KIND_FASTSCAN, KIND_MULTIBUCKET, KIND_RANK = 1, 2, 3, 4, 5, 6
 
 
 class OrdvecError(ValueError):
@@ -94,6 +94,7 @@ SIGNATURES = {
     "ovb_bitmap_new": (S, [U32, U32, PP]),
     "ovb_fastscan_new": (S, [U32, PP]),
     "ovb_multibucket_new": (S, [U32, U32, PP]),
+    "ovb_rank_new": (S, [U32, PP]),
     "ovb_index_add": (S, [P, P, U64]),
     "ovb_index_add_device": (S, [P, P, U64]),
     "ovb_index_load_any": (S, [C.c_char_p, U64, PP]),
@@ -117,6 +118,9 @@ SIGNATURES = {
     "ovb_synth_docs": (S, [U64, U64, U64, U32, F, P]),
     "ovb_synth_queries": (S, [U64, U64, U64, U32, F, F, P, P]),
     "ovb_rankquant_search_split": (S, [P, P, U64, U64, U32, P, P]),
+    "ovb_rankquant_search_symmetric": (S, [P, P, U64, U64, P, P]),
+    "ovb_rank_search": (S, [P, P, U64, U64, P, P]),
+    "ovb_rank_search_asymmetric": (S, [P, P, U64, U64, P, P]),
     "ovb_rankquant_search_mixed": (S, [P, U32, P, P, P, U64, U64, P, P]),
     "ovb_mixed_plan_info": (S, [P, U64, U64, P, P, P]),
     "ovb_server_new": (S, [P, P]),

@@ -18,7 +18,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _lib as _lib_mod
-from ._lib import (KIND_BITMAP, KIND_FASTSCAN, KIND_MULTIBUCKET, KIND_RANK_QUANT, KIND_SIGN_BITMAP,
+from ._lib import (KIND_BITMAP, KIND_FASTSCAN, KIND_MULTIBUCKET, KIND_RANK, KIND_RANK_QUANT, KIND_SIGN_BITMAP,
                    IndexInfo, OrdvecError, check, lib)
 
 
@@ -157,15 +157,48 @@ def _new(fn, *args):
 
 
 def load(path: str):
-    """Load any of .ovrq / .ovbm / .ovsb / .ovfs into HBM (src/rank_io.rs)."""
+    """Load any of .ovrq / .ovbm / .ovsb / .ovfs / .ovr into HBM (src/rank_io.rs)."""
     h = C.c_void_p()
     check(lib().ovb_index_load_any(str(path).encode(), 0, C.byref(h)))
     info = IndexInfo()
     lib().ordvec_index_info_init(C.byref(info))
     check(lib().ordvec_index_info(h, C.byref(info)))
     cls = {KIND_RANK_QUANT: RankQuant, KIND_BITMAP: Bitmap, KIND_SIGN_BITMAP: SignBitmap,
-           KIND_FASTSCAN: RankQuantFastscan}[info.kind]
+           KIND_FASTSCAN: RankQuantFastscan, KIND_RANK: Rank}[info.kind]
     return cls._wrap_loaded(h)
+
+
+def _full_search(fn, h, n: int, dim: int, queries, k: int) -> SearchResults:
+    """nq x min(k, n) results of one of the library's full searches."""
+    q = _rows(queries, dim)
+    nq = q.size // dim
+    ke = min(k, n)
+    s = np.empty(max(nq * ke, 1), np.float32)
+    i = np.empty(max(nq * ke, 1), np.int64)
+    check(fn(h, _ptr(q), nq, ke, _ptr(s), _ptr(i)))
+    return SearchResults(s[: nq * ke], i[: nq * ke], nq, ke)
+
+
+class Rank(_Index):
+    """Full-precision rank index: one u16 rank per coordinate (src/rank.rs:283-482)."""
+
+    def __init__(self, dim: int):
+        super().__init__(_new(lib().ovb_rank_new, dim))
+
+    @classmethod
+    def load(cls, path: str) -> "Rank":
+        obj = load(path)
+        if not isinstance(obj, Rank):
+            raise OrdvecError(4, "not a Rank index")
+        return obj
+
+    def search(self, queries, k: int) -> SearchResults:
+        """Symmetric rank-cosine (Spearman) search, src/rank.rs:364-419."""
+        return _full_search(lib().ovb_rank_search, self._h, len(self), self.dim, queries, k)
+
+    def search_asymmetric(self, queries, k: int) -> SearchResults:
+        """L2-normalised f32 query against the stored ranks, src/rank.rs:420-482."""
+        return _full_search(lib().ovb_rank_search_asymmetric, self._h, len(self), self.dim, queries, k)
 
 
 class RankQuant(_Index):
@@ -184,6 +217,10 @@ class RankQuant(_Index):
         if not isinstance(obj, RankQuant):
             raise OrdvecError(4, "not a RankQuant index")
         return obj
+
+    def search(self, queries, k: int) -> SearchResults:
+        """Symmetric search (src/quant.rs:629-695): the query is rank-bucketed like a document."""
+        return _full_search(lib().ovb_rankquant_search_symmetric, self._h, len(self), self.dim, queries, k)
 
     def search_asymmetric(self, queries, k: int) -> SearchResults:
         """src/quant.rs:713-847: nq x min(k, n), (score desc, id asc)."""

@@ -69,6 +69,7 @@ uint32_t encode_kind(uint32_t kind) {
     case OVB_INDEX_KIND_SIGN_BITMAP: return 1;
     case ORDVEC_INDEX_KIND_BITMAP: return 2;
     case OVB_INDEX_KIND_FASTSCAN: return 3;
+    case OVB_INDEX_KIND_RANK: return 5;
     default: return 4;
   }
 }
@@ -503,6 +504,17 @@ ordvec_status_t ovb_multibucket_new(uint32_t dim, uint32_t bits, ordvec_index_t*
   });
 }
 
+ordvec_status_t ovb_rank_new(uint32_t dim, ordvec_index_t** out) {
+  return boundary([&] {
+    if (!out) fail(ORDVEC_STATUS_NULL_POINTER, "out pointer is NULL");
+    *out = nullptr;
+    // Rank::new (src/rank.rs:316-324)
+    if (dim < 2) fail(ORDVEC_STATUS_BAD_ARGUMENT, "dim must be >= 2");
+    if (dim > 65535) fail(ORDVEC_STATUS_BAD_ARGUMENT, "dim must fit in u16");
+    *out = (ordvec_index_t*)new_index(OVB_INDEX_KIND_RANK, dim, 16, 0);
+  });
+}
+
 ordvec_status_t ovb_index_add(ordvec_index_t* index, const float* vectors, uint64_t n) {
   return boundary([&] {
     Index& ix = as_index_mut(index);
@@ -749,6 +761,41 @@ ordvec_status_t ovb_fastscan_search(const ordvec_index_t* fs, const float* queri
     const float* d_q = upload_queries(w, queries, nq, ix.dim, true);
     uint32_t got = engine_fastscan_full(ix, d_q, nq, ke, w, w.stream);
     download_results(w, nq * got, 0, 0, scores, ids);
+  });
+}
+
+// Full searches whose query is rank-transformed on the device.
+static void rank_query_search(const ordvec_index_t* h, uint32_t kind, const char* what, const float* queries,
+                              uint64_t nq, uint64_t k, float* scores, int64_t* ids, int variant) {
+  const Index& ix = as_index(h);
+  if (ix.kind != kind) fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, std::string("not a ") + what + " index");
+  need_queries(queries, nq);
+  const uint64_t ke = k < ix.n ? k : ix.n;
+  if (!ke || !nq) return;
+  if (!scores || !ids) fail(ORDVEC_STATUS_NULL_POINTER, "output pointer is NULL");
+  if (ix.dim > kMaxDeviceRankDim)  // the rank transform and the scans' shared-memory query row
+    fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "device rank search supports dim <= 16384");
+  Workspace& w = workspace();
+  const float* d_q = upload_queries(w, queries, nq, ix.dim, true);
+  uint32_t got = variant == 2 ? engine_rankquant_symmetric(ix, d_q, nq, ke, w, w.stream)
+                              : engine_rank_full(ix, d_q, nq, ke, variant == 1, w, w.stream);
+  download_results(w, nq * got, 0, 0, scores, ids);
+}
+
+ordvec_status_t ovb_rank_search(const ordvec_index_t* rank, const float* queries, uint64_t nq, uint64_t k,
+                                float* scores, int64_t* ids) {
+  return boundary([&] { rank_query_search(rank, OVB_INDEX_KIND_RANK, "Rank", queries, nq, k, scores, ids, 0); });
+}
+
+ordvec_status_t ovb_rank_search_asymmetric(const ordvec_index_t* rank, const float* queries, uint64_t nq,
+                                           uint64_t k, float* scores, int64_t* ids) {
+  return boundary([&] { rank_query_search(rank, OVB_INDEX_KIND_RANK, "Rank", queries, nq, k, scores, ids, 1); });
+}
+
+ordvec_status_t ovb_rankquant_search_symmetric(const ordvec_index_t* rq, const float* queries, uint64_t nq,
+                                               uint64_t k, float* scores, int64_t* ids) {
+  return boundary([&] {
+    rank_query_search(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "RankQuant", queries, nq, k, scores, ids, 2);
   });
 }
 

@@ -11,6 +11,9 @@
 //   3 FastScan    b=2 buckets, nibble (b[2p]<<2)|b[2p+1] (src/fastscan.rs:87-110),
 //                 written straight into the device block layout (scan_fastscan.cu)
 //   4 MultiBucket one bitmap per bucket (src/multi_bucket.rs:95-117)
+//   5 Rank        the u16 rank itself (src/rank.rs:340-354)
+//   6 symmetric RankQuant query: bucket_centre(bucket) as f32, the query side
+//                 of RankQuant::search's LUT (src/quant.rs:660-669)
 #include "ovb_common.cuh"
 #include "ovb_kernels.h"
 
@@ -94,6 +97,14 @@ __global__ void rank_encode_kernel(int kind, const float* __restrict__ vecs, uin
       }
       o[(g * 32 + lane) * 16 + b] = (uint8_t)(nib[0] | (nib[1] << 4));
     }
+  } else if (kind == 5) {
+    uint16_t* o = (uint16_t*)out + doc * dim;
+    for (uint32_t j = threadIdx.x; j < dim; j += blockDim.x) o[j] = rank[j];
+  } else if (kind == 6) {
+    float* o = (float*)out + doc * dim;
+    const float centre = ((float)(1u << bits) - 1.0f) / 2.0f;
+    for (uint32_t j = threadIdx.x; j < dim; j += blockDim.x)
+      o[j] = (float)(uint32_t)(((uint64_t)rank[j] << bits) / dim) - centre;
   } else {  // kind 4
     const uint32_t qpb = dim / 64, nb = 1u << bits;
     uint64_t* o = (uint64_t*)out + doc * (uint64_t)nb * qpb;

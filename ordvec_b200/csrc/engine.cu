@@ -26,11 +26,12 @@ uint64_t keys_budget() {
 }
 
 // rankquant_norm (src/rank.rs:275-280) and 1/norm in f32, as the reference.
-float inv_rankquant_norm(uint32_t dim, uint32_t bits) {
+float rankquant_norm_f32(uint32_t dim, uint32_t bits) {
   const double n = (double)(1u << bits);
-  const float norm = (float)std::sqrt((double)dim * ((n * n - 1.0) / 12.0));
-  return 1.0f / norm;
+  return (float)std::sqrt((double)dim * ((n * n - 1.0) / 12.0));
 }
+
+float inv_rankquant_norm(uint32_t dim, uint32_t bits) { return 1.0f / rankquant_norm_f32(dim, bits); }
 
 void select_rows(Workspace& w, const uint32_t* keys, const uint32_t* ids, const uint64_t* row_off,
                  uint64_t ld, uint64_t n, uint64_t rows, uint32_t k, uint32_t key_bits,
@@ -444,6 +445,56 @@ uint32_t engine_rankquant_full(const Index& rq, const float* d_q, uint64_t nq, u
     launch_asym_scan(rq.codes.as<uint8_t>(), rq.n, rq.dim, rq.bits, qu + q0 * rq.dim, qn, inv_norm, keys,
                      rq.n, st);
   });
+  return ke;
+}
+
+// RankQuant::search (src/quant.rs:629-695).  Query side of the LUT =
+// bucket_centre(bucket(rank)), a half-integer; each LUT entry is a multiple of
+// 1/4 and for b <= 4 every partial sum stays below 2^22 quarters, so the
+// reference's sequential f32 sum is exact and equals the asymmetric scan's
+// FP64 dot; (float)(dot * (double)inv_norm_sq) is then the reference's single
+// f32 rounding of acc * inv_norm_sq (a product of two f32 is exact in f64).
+uint32_t engine_rankquant_symmetric(const Index& rq, const float* d_q, uint64_t nq, uint64_t k, Workspace& w,
+                                    cudaStream_t st) {
+  require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "search");
+  const uint32_t ke = (uint32_t)(k < rq.n ? k : rq.n);
+  if (!ke || !nq) return ke;
+  float* qc = (float*)w.q_unit.ensure(nq * rq.dim * 4);
+  launch_encode(6, d_q, nq, rq.dim, rq.bits, 0, 0, qc, 0, st);
+  const float norm = rankquant_norm_f32(rq.dim, rq.bits);
+  const float inv_norm_sq = 1.0f / (norm * norm);
+  uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
+  uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
+  full_scan_select(w, nq, rq.n, ke, 32, ok, oi, st, [&](uint64_t q0, uint64_t qn, uint32_t* keys) {
+    launch_asym_scan(rq.codes.as<uint8_t>(), rq.n, rq.dim, rq.bits, qc + q0 * rq.dim, qn, inv_norm_sq, keys, rq.n,
+                     st);
+  });
+  return ke;
+}
+
+// Rank::search / Rank::search_asymmetric (src/rank.rs:364-482).
+uint32_t engine_rank_full(const Index& rk, const float* d_q, uint64_t nq, uint64_t k, bool asymmetric, Workspace& w,
+                          cudaStream_t st) {
+  require_kind(rk, OVB_INDEX_KIND_RANK, asymmetric ? "search_asymmetric" : "search");
+  const uint32_t ke = (uint32_t)(k < rk.n ? k : rk.n);
+  if (!ke || !nq) return ke;
+  const uint16_t* ranks = rk.codes.as<uint16_t>();
+  const uint32_t dim = rk.dim;
+  uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
+  uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
+  if (asymmetric) {
+    const float* qu = normalised(w, d_q, nq, dim, st);
+    float* qsum = (float*)w.invq.ensure(nq * 4);
+    full_scan_select(w, nq, rk.n, ke, 32, ok, oi, st, [&](uint64_t q0, uint64_t qn, uint32_t* keys) {
+      launch_rank_asym_scan(ranks, rk.n, dim, qu + q0 * dim, qsum + q0, qn, keys, rk.n, st);
+    });
+  } else {
+    uint16_t* qr = (uint16_t*)w.qbits.ensure(nq * dim * 2);
+    launch_encode(5, d_q, nq, dim, 0, 0, 0, qr, 0, st);
+    full_scan_select(w, nq, rk.n, ke, 32, ok, oi, st, [&](uint64_t q0, uint64_t qn, uint32_t* keys) {
+      launch_rank_sym_scan(ranks, rk.n, dim, qr + q0 * dim, qn, keys, rk.n, st);
+    });
+  }
   return ke;
 }
 

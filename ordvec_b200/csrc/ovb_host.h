@@ -149,6 +149,12 @@ uint32_t engine_rankquant_split_fixed(const Index& rq, const float* d_q, uint64_
 uint32_t engine_rankquant_subset(const Index& rq, const float* d_q, uint64_t nq,
                                  const uint64_t* d_off, const uint32_t* d_cands, uint64_t max_row,
                                  uint64_t k, Workspace& w, cudaStream_t st);
+// RankQuant::search (symmetric: the query is rank-bucketed like a document)
+uint32_t engine_rankquant_symmetric(const Index& rq, const float* d_q, uint64_t nq, uint64_t k, Workspace& w,
+                                    cudaStream_t st);
+// Rank::search (asymmetric = false) / Rank::search_asymmetric
+uint32_t engine_rank_full(const Index& rk, const float* d_q, uint64_t nq, uint64_t k, bool asymmetric, Workspace& w,
+                          cudaStream_t st);
 uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint64_t m,
                            const float* d_weights, Workspace& w, cudaStream_t st,
                            const float* q_unit = nullptr);

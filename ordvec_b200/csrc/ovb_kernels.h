@@ -131,6 +131,15 @@ void launch_rank_filter_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint3
 void launch_split_margin(const uint32_t* sel_keys, uint64_t nq, uint32_t kp, uint32_t k, const float* l1,
                          float bound_per_l1, uint32_t* flag, cudaStream_t stream);
 
+// ---- K9 Rank (u16) index scans (scan_rank_full.cu) -> key32 [nq][ld] ------------
+float rank_norm_f32(uint32_t dim);
+// Rank::search: q_ranks = the queries' u16 ranks (nq x dim)
+void launch_rank_sym_scan(const uint16_t* ranks, uint64_t n, uint32_t dim, const uint16_t* q_ranks, uint64_t nq,
+                          uint32_t* keys, uint64_t ld, cudaStream_t stream);
+// Rank::search_asymmetric: q_unit rows; q_sum (nq floats) is scratch the launch fills
+void launch_rank_asym_scan(const uint16_t* ranks, uint64_t n, uint32_t dim, const float* q_unit, float* q_sum,
+                           uint64_t nq, uint32_t* keys, uint64_t ld, cudaStream_t stream);
+
 // ---- K4/K5 asymmetric RankQuant scoring (scan_asym.cu) ---------------------------
 void launch_asym_scan(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_t bits,
                       const float* q_unit, uint64_t nq, float inv_norm, uint32_t* keys,

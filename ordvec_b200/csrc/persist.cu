@@ -5,11 +5,13 @@
 //   OVBM/TVBM  magic | ver u8 | dim u32 | n_top u32 | n u32     (17 B)  Bitmap
 //   OVSB/TVSB  magic | ver u8 | dim u32 | n u32                 (13 B)  SignBitmap
 //   OVFS       magic | ver u8 | dim u32 | n u32                 (13 B)  FastScan
-//   OVR1/TVR1  Rank: recognised, not loadable (not a scan format)
+//   OVR1/TVR1  magic | ver u8 | dim u32 | n u32                 (13 B)  Rank (u16 LE ranks;
+//              ABI v1's loader refuses it as an unsupported format)
 // The loaders replay the reference's validation in the same order
 // (header domains, MAX_VECTORS, 128 GiB payload cap, exact payload length,
 // then row invariants: RankQuant constant composition, Bitmap popcount ==
-// n_top, FastScan nibble domain / composition / zero tail padding).
+// n_top, FastScan nibble domain / composition / zero tail padding, Rank rows
+// permutations of [0, dim)).
 // Malformed files map to CORRUPT_INDEX, I/O failures to IO, known-but-not-v1
 // formats to UNSUPPORTED_FORMAT (ordvec-ffi/src/lib.rs:241-250, 697-776).
 #include <sys/stat.h>
@@ -192,6 +194,26 @@ void validate_rankquant_rows(const std::vector<uint8_t>& p, const Header& h) {
   }
 }
 
+// load_rank_from_stream (src/rank_io.rs:581-633): every row a permutation of
+// [0, dim); a stamp per value marks the row that last held it.
+void validate_rank_rows(const std::vector<uint8_t>& p, const Header& h) {
+  std::vector<uint32_t> seen(h.dim, 0);
+  for (uint64_t r = 0; r < h.n; r++) {
+    const uint32_t stamp = (uint32_t)r + 1;
+    for (uint64_t j = 0; j < h.dim; j++) {
+      const uint8_t* b = p.data() + (r * h.dim + j) * 2;
+      const uint32_t v = (uint32_t)b[0] | ((uint32_t)b[1] << 8);
+      if (v >= h.dim)
+        corrupt("OVR1 rank value " + std::to_string(v) + " >= dim (" + std::to_string(h.dim) +
+                "); ranks must be a permutation of [0, dim)");
+      if (seen[v] == stamp)
+        corrupt("OVR1 row " + std::to_string(r) + " is not a permutation of [0, dim): value " + std::to_string(v) +
+                " repeats");
+      seen[v] = stamp;
+    }
+  }
+}
+
 void validate_bitmap_rows(const std::vector<uint8_t>& p, const Header& h) {
   const uint64_t qpv = h.dim / 64;
   const uint64_t* w = (const uint64_t*)p.data();
@@ -240,6 +262,8 @@ uint64_t Index::ref_bytes_per_vec() const {
       return dim / 2;
     case OVB_INDEX_KIND_MULTIBUCKET:
       return (uint64_t)nb() * dim / 8;
+    case OVB_INDEX_KIND_RANK:
+      return (uint64_t)dim * 2;
   }
   return 0;
 }
@@ -255,6 +279,8 @@ uint64_t Index::device_bytes(uint64_t rows) const {
       return ((rows + 31) / 32) * fastscan_block_bytes(pairs_pad);
     case OVB_INDEX_KIND_MULTIBUCKET:
       return rows * nb() * (dim / 64) * 8;
+    case OVB_INDEX_KIND_RANK:
+      return rows * dim * 2;
   }
   return 0;
 }
@@ -284,8 +310,7 @@ std::unique_ptr<Index> load_index_file(const char* path, bool v1_only) {
   f.read(m, 4, "ordvec index", "magic");
   const Fmt fmt = lookup_magic(m);
   if (fmt == Fmt::Unknown) corrupt("unrecognized ordvec index magic");
-  if (fmt == Fmt::Rank) fail(ORDVEC_STATUS_UNSUPPORTED_FORMAT, "ABI v1 supports only RankQuant and Bitmap indexes");
-  if (v1_only && fmt == Fmt::Sign)
+  if (v1_only && (fmt == Fmt::Rank || fmt == Fmt::Sign))
     fail(ORDVEC_STATUS_UNSUPPORTED_FORMAT, "ABI v1 supports only RankQuant and Bitmap indexes");
   if (v1_only && fmt == Fmt::FastScan)
     fail(ORDVEC_STATUS_UNSUPPORTED_FORMAT, "ABI v1 does not support RankQuantFastscan indexes");
@@ -298,6 +323,11 @@ std::unique_ptr<Index> load_index_file(const char* path, bool v1_only) {
   ix->n = h.n;
   ix->file_size = f.size;
   switch (h.fmt) {
+    case Fmt::Rank:
+      validate_rank_rows(payload, h);
+      ix->kind = OVB_INDEX_KIND_RANK;
+      ix->bits = 16;
+      break;
     case Fmt::RankQuant:
       validate_rankquant_rows(payload, h);
       ix->kind = ORDVEC_INDEX_KIND_RANK_QUANT;
@@ -403,6 +433,11 @@ void write_index_file(const Index& ix, const char* path) {
       break;
     case OVB_INDEX_KIND_FASTSCAN:
       hdr = {'O', 'V', 'F', 'S', 1};
+      put32(ix.dim);
+      put32((uint32_t)ix.n);
+      break;
+    case OVB_INDEX_KIND_RANK:
+      hdr = {'O', 'V', 'R', '1', 1};
       put32(ix.dim);
       put32((uint32_t)ix.n);
       break;

@@ -226,3 +226,71 @@ def test_multibucket_diag_weights_are_integer_overlaps(orc):
     codes = np.stack([orc.unpack_buckets(rq[r * dim * bits // 8:(r + 1) * dim * bits // 8], dim, bits) for r in range(21)])
     agree = (codes[1:] == codes[0][None]).sum(axis=1)
     assert np.array_equal(s, agree.astype(np.float32))
+
+
+def test_rank_and_symmetric_ties_return_lowest_row_ids(orc):
+    """tests/determinism_contract.rs:15-38: Rank::search and RankQuant::search
+    (symmetric) on 8 identical docs return rows 0..3; Rank::search_asymmetric
+    with a zero query scores every doc 0.0."""
+    dim = 64
+    docs = np.ones((8, dim), np.float32)
+    ranks = orc.rank_encode(docs, dim)
+    _, i = orc.rank_search(ranks, 8, dim, np.ones(dim, np.float32), 4)
+    assert i[0].tolist() == [0, 1, 2, 3]
+    s, i = orc.rank_search(ranks, 8, dim, np.zeros(dim, np.float32), 4, asymmetric=True)
+    assert i[0].tolist() == [0, 1, 2, 3] and (s == 0.0).all()
+    packed = orc.rankquant_encode(docs, dim, 2)
+    _, i = orc.rq_search_sym(packed, 8, dim, 2, np.ones(dim, np.float32), 4)
+    assert i[0].tolist() == [0, 1, 2, 3]
+
+
+def test_rank_persisted_payload_golden_bytes(orc):
+    """tests/persistence_compat.rs:101-104: Rank::new(4) of [0, 1, 2, 3] stores
+    the u16 ranks 0 1 2 3 (payload bytes 0 0 1 0 2 0 3 0)."""
+    r = orc.rank_encode(np.arange(4, dtype=np.float32), 4)
+    assert r.view(np.uint8).tolist() == [0, 0, 1, 0, 2, 0, 3, 0]
+
+
+def test_rank_scores_are_spearman_and_centred_cosine(orc):
+    """Rank::search is the Spearman correlation of the two rank vectors and
+    Rank::search_asymmetric the cosine of the unit query with the centred ranks
+    (src/rank.rs:356-482), checked against numpy in float64."""
+    rng = np.random.default_rng(7)
+    dim, n = 96, 40
+    docs = rng.standard_normal((n, dim)).astype(np.float32)
+    q = rng.standard_normal(dim).astype(np.float32)
+    ranks = orc.rank_encode(docs, dim).reshape(n, dim).astype(np.float64)
+    qr = np.argsort(np.argsort(q, kind="stable"), kind="stable").astype(np.float64)
+    s, i = orc.rank_search(ranks.astype(np.uint16), n, dim, q, n)
+    rho = np.array([np.corrcoef(qr, ranks[d])[0, 1] for d in range(n)])
+    assert np.allclose(s[0], rho[i[0]], atol=1e-6)
+    s, i = orc.rank_search(ranks.astype(np.uint16), n, dim, q, n, asymmetric=True)
+    qu = q.astype(np.float64) / np.linalg.norm(q.astype(np.float64))
+    cen = ranks - (dim - 1) / 2.0
+    cos = cen @ qu / np.sqrt(dim * (dim * dim - 1) / 12.0)
+    assert np.allclose(s[0], cos[i[0]], atol=1e-5)
+
+
+def test_rankquant_symmetric_scores_are_exact_centre_products(orc):
+    """RankQuant::search (src/quant.rs:629-695): the LUT sum of
+    centre(q_bucket) * centre(d_bucket) is a multiple of 1/4 below 2^22 quarters,
+    so the f32 score is exactly f32(sum) * f32(1 / norm^2), one rounding."""
+    rng = np.random.default_rng(8)
+    dim, n = 128, 50
+    docs = rng.standard_normal((n, dim)).astype(np.float32)
+    q = rng.standard_normal(dim).astype(np.float32)
+    for bits in (1, 2, 4):
+        packed = orc.rankquant_encode(docs, dim, bits)
+        s, i = orc.rq_search_sym(packed, n, dim, bits, q, n)
+        codes = np.stack([orc.unpack_buckets(packed[r * dim * bits // 8:(r + 1) * dim * bits // 8], dim, bits)
+                          for r in range(n)]).astype(np.float64)
+        qb = orc.unpack_buckets(orc.rankquant_encode(q, dim, bits), dim, bits).astype(np.float64)
+        c = ((1 << bits) - 1) / 2.0
+        dot = (codes - c) @ (qb - c)
+        nb = float(1 << bits)
+        norm = np.float32(np.sqrt(dim * ((nb * nb - 1.0) / 12.0)))
+        inv_sq = np.float32(1.0) / (norm * norm)
+        want = (dot.astype(np.float32) * inv_sq).astype(np.float32)
+        assert np.array_equal(s[0], want[i[0]]), bits
+        order = sorted(range(n), key=lambda d: (-want[d], d))
+        assert i[0].tolist() == order, bits
