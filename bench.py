@@ -349,6 +349,66 @@ def large_run(ob, torch, dev, steps: int, plain_queries: int):
     return out
 
 
+# ----------------------------------------------------- Rank and symmetric
+def rank_modes_run(ob, torch, dev, rq, queries, plain_queries: int):
+    """The Rank (u16) index and RankQuant's symmetric search, device-timed
+    through ob.search_device: Rank(768) over N=1,000,000 synthetic docs
+    (1.54 GB of ranks) and this benchmark's RankQuant b=2 index, one query per
+    call (plain) and a batch per call.  For the plain calls the whole call's
+    time is set against the bytes the scan must read (ranks or codes once, plus
+    the 4-byte key row), a lower bound on the scan kernel's HBM rate."""
+    hbm_peak, _, peak_kind = measured_peaks()
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    out = {}
+
+    def timed(ix, d_q, nq, k, asym, reps):
+        d_s = torch.empty(nq * k, dtype=torch.float32, device=dev)
+        d_i = torch.empty(nq * k, dtype=torch.int64, device=dev)
+        run = lambda qp: ob.search_device(ix, qp, nq, k, d_s.data_ptr(), d_i.data_ptr(), sp, asymmetric=asym)
+        for r in range(3):
+            run(d_q[r * nq].data_ptr() if nq == 1 else d_q.data_ptr())
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        for r in range(reps):
+            ev[r][0].record(stream)
+            run(d_q[r * nq].data_ptr() if nq == 1 else d_q.data_ptr())
+            ev[r][1].record(stream)
+        torch.cuda.synchronize(dev)
+        return [a.elapsed_time(b) for a, b in ev]
+
+    def roof(nbytes, ms):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        return {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
+                "peak_source": f"{peak_kind} HBM copy"}
+
+    n, dim, k, nb = 1_000_000, 768, 100, 64
+    rk = ob.Rank(dim)
+    for first in range(0, n, 250_000):
+        rk.add(ob.synth_docs(0x0DD5EED6, 250_000, dim, first=first))
+    q, _ = ob.synth_queries(0x0DD5EED7, n, nb, dim)
+    d_q = torch.from_numpy(q).to(dev)
+    P = max(4, min(plain_queries, 32))
+    for asym in (False, True):
+        plain = timed(rk, d_q, 1, k, asym, P)
+        batch = timed(rk, d_q, nb, k, asym, 3)
+        out["rank_asymmetric" if asym else "rank_symmetric"] = {
+            "workload": f"Rank dim={dim} N={n} top-{k}", "plain_qps": 1e3 / statistics.mean(plain),
+            "plain_p50_ms": float(np.percentile(plain, 50)), "batched_qps": nb / (statistics.median(batch) * 1e-3),
+            "batch_queries": nb, "roofline_plain_call": roof(n * dim * 2 + 4 * n, statistics.median(plain))}
+    del rk
+    nr = len(rq)
+    d_q = torch.from_numpy(queries).to(dev)
+    plain = timed(rq, d_q, 1, 10, False, P)
+    nbq = min(1000, d_q.shape[0])
+    batch = timed(rq, d_q, nbq, 10, False, 3)
+    out["rankquant_symmetric"] = {
+        "workload": f"RankQuant b={rq.bits} dim={rq.dim} N={nr} (this benchmark's corpus) symmetric top-10",
+        "plain_qps": 1e3 / statistics.mean(plain), "plain_p50_ms": float(np.percentile(plain, 50)),
+        "batched_qps": nbq / (statistics.median(batch) * 1e-3), "batch_queries": nbq,
+        "roofline_plain_call": roof(nr * rq.dim * rq.bits // 8 + 4 * nr, statistics.median(plain))}
+    return out
+
+
 # ------------------------------------------------------------------ serving
 def serving_run(ob, rq, fs, queries, batched_ids, seconds: float, rate_qps: float):
     """The serving loop on this workload's route: seeded Poisson request
@@ -411,6 +471,8 @@ def profile_case(case: str):
       popc      the same index, one query per call (popc_rows_kernel, wide select)
       rank      RankQuant(1024, 2) exact top-100 of 1024 queries, N=1M (rank_tc_kernel)
       fastscan  this workload's FastScan top-1000 of 1000 queries (fastscan_tc_kernel)
+      rankfull  Rank(768) N=1M top-100: symmetric then asymmetric, 1 query and 64
+                queries per call (rank_tile_kernel)
     Each search runs more than once so captures can skip the first call."""
     import ordvec_b200 as ob
 
@@ -435,6 +497,16 @@ def profile_case(case: str):
         q, _ = ob.synth_queries(SEED + 1, N_DOCS, NQ, DIM)
         for _ in range(2):
             fs.search(q, M)
+    elif case == "rankfull":
+        n = 1_000_000
+        rk = ob.Rank(768)
+        for first in range(0, n, 250_000):
+            rk.add(ob.synth_docs(0x0DD5EED6, 250_000, 768, first=first))
+        q, _ = ob.synth_queries(0x0DD5EED7, n, 64, 768)
+        for fn in (rk.search, rk.search_asymmetric):
+            for _ in range(2):
+                fn(q[:1], 100)
+                fn(q, 100)
     else:
         raise SystemExit(f"unknown profile case {case}")
     print(f"profile case {case}: done", flush=True)
@@ -555,7 +627,7 @@ def main():
                          "0 = skip, -1 = 4096 on a single GPU")
     ap.add_argument("--large", default="auto", choices=["auto", "on", "off"],
                     help="also run the N=10M dim-768 bitmap / multi-bucket configuration (auto: one GPU only)")
-    ap.add_argument("--profile-case", choices=["bitmap", "popc", "rank", "fastscan"],
+    ap.add_argument("--profile-case", choices=["bitmap", "popc", "rank", "fastscan", "rankfull"],
                     help="run one small kernel workload for an ncu capture and exit")
     args = ap.parse_args()
     if args.profile_case:
@@ -723,6 +795,7 @@ def main():
         "sign_b1_plain": sign_plain_run(ob, torch, dev, args.plain_queries, not args.no_cpu) if world == 1 else None,
         "serving_multi": serving_multi_run(ob, args.serve_seconds, [20_000.0, 100_000.0, args.serve_rate])
         if world == 1 and args.serve_seconds > 0 else None,
+        "rank_modes": rank_modes_run(ob, torch, dev, rq, queries, args.plain_queries) if world == 1 else None,
         "large_corpus": large_run(ob, torch, dev, args.steps, args.plain_queries)
         if args.large == "on" or (args.large == "auto" and world == 1) else None,
         "stages_ms": dict(zip(STAGES, stages)),

@@ -191,6 +191,17 @@ ordvec_status_t ovb_rankquant_search(const ordvec_index_t *rq, const float *quer
 ordvec_status_t ovb_rankquant_search_split(const ordvec_index_t *rq, const float *queries,
                                            uint64_t nq, uint64_t k, uint32_t exact,
                                            float *scores, int64_t *ids);
+/* Full searches on device buffers, stream-ordered on `stream` (a
+ * cudaStream_t; queries nq x dim f32, results nq x min(k, n) as in the host
+ * entry points; query finiteness is the caller's responsibility).  method
+ * OVB_SEARCH_DEFAULT is the kind's `search` (RankQuant and Rank: symmetric;
+ * Bitmap; RankQuantFastscan), OVB_SEARCH_ASYMMETRIC its `search_asymmetric`
+ * (RankQuant, Rank).  Calls from one thread share its workspace and must be
+ * ordered on one stream. */
+#define OVB_SEARCH_DEFAULT 0u
+#define OVB_SEARCH_ASYMMETRIC 1u
+ordvec_status_t ovb_index_search_device(const ordvec_index_t *index, uint32_t method, const float *d_queries,
+                                        uint64_t nq, uint64_t k, float *d_scores, int64_t *d_ids, void *stream);
 /* RankQuant::search, symmetric (src/quant.rs:629-695): the query is
  * rank-transformed and bucketed like a document; score = sum_d
  * centre(q_bucket) * centre(d_bucket) / norm^2, the reference's values bit for

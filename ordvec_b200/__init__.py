@@ -6,11 +6,11 @@ Device-resident indices and CUDA kernels behind the reference's C ABI
 from ._lib import LIB_PATH, OrdvecError, lib
 from .api import (Bitmap, CandidateBatch, MultiBucketBitmap, Rank, RankQuant, RankQuantFastscan,
                   SearchResults, Server, SignBitmap, Ticket, TwoStageCandidatePolicy, last_launch_count, load,
-                  set_device, synth_docs, synth_queries, two_stage_profile, two_stage_search,
+                  search_device, set_device, synth_docs, synth_queries, two_stage_profile, two_stage_search,
                   two_stage_search_device, search_mixed, mixed_plan_info)
 
 __all__ = [
     "Bitmap", "CandidateBatch", "MultiBucketBitmap", "OrdvecError", "Rank", "RankQuant", "RankQuantFastscan",
     "SearchResults", "SignBitmap", "TwoStageCandidatePolicy", "LIB_PATH", "last_launch_count", "lib",
-    "load", "synth_docs", "synth_queries", "two_stage_search", "Server", "Ticket", "search_mixed", "mixed_plan_info",
+    "load", "search_device", "synth_docs", "synth_queries", "two_stage_search", "Server", "Ticket", "search_mixed", "mixed_plan_info",
 ]

@@ -591,6 +591,15 @@ def two_stage_search_device(rq: RankQuant, stage1: _Index, d_queries: int, nq: i
                                             C.c_void_p(d_scores), C.c_void_p(d_ids), C.c_void_p(stream)))
 
 
+def search_device(index: _Index, d_queries: int, nq: int, k: int, d_scores: int, d_ids: int, stream: int,
+                  asymmetric: bool = False) -> None:
+    """Device-pointer full search, asynchronous on `stream` (cudaStream_t as int):
+    the index's `search` (RankQuant / Rank symmetric, Bitmap, RankQuantFastscan),
+    or `search_asymmetric` (RankQuant, Rank) with asymmetric=True."""
+    check(lib().ovb_index_search_device(index.handle, 1 if asymmetric else 0, C.c_void_p(d_queries), nq, k,
+                                        C.c_void_p(d_scores), C.c_void_p(d_ids), C.c_void_p(stream)))
+
+
 def two_stage_profile(rq: RankQuant, stage1: _Index, d_queries: int, nq: int, m: int, k: int,
                       d_scores: int, d_ids: int, stream: int) -> List[float]:
     """Synchronous device-pointer two-stage search returning per-stage device ms:

@@ -842,6 +842,47 @@ ordvec_status_t ovb_two_stage_search_device(const ordvec_index_t* rq, const ordv
   });
 }
 
+ordvec_status_t ovb_index_search_device(const ordvec_index_t* index, uint32_t method, const float* d_queries,
+                                        uint64_t nq, uint64_t k, float* d_scores, int64_t* d_ids, void* stream) {
+  return boundary([&] {
+    const Index& ix = as_index(index);
+    need_queries(d_queries, nq);
+    const bool asym = method == OVB_SEARCH_ASYMMETRIC;
+    if (method != OVB_SEARCH_DEFAULT && !asym) fail(ORDVEC_STATUS_BAD_ARGUMENT, "method must be 0 or 1");
+    const bool rank_kind = ix.kind == ORDVEC_INDEX_KIND_RANK_QUANT || ix.kind == OVB_INDEX_KIND_RANK;
+    if (!rank_kind && (asym || (ix.kind != ORDVEC_INDEX_KIND_BITMAP && ix.kind != OVB_INDEX_KIND_FASTSCAN)))
+      fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "this index kind has no such full search");
+    if (ix.kind == OVB_INDEX_KIND_RANK && ix.dim > kMaxDeviceRankDim)
+      fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "device rank search supports dim <= 16384");
+    if (ix.kind == ORDVEC_INDEX_KIND_RANK_QUANT && !asym && ix.dim > kMaxDeviceRankDim)
+      fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "device rank transform supports dim <= 16384");
+    const uint64_t ke = k < ix.n ? k : ix.n;
+    if (!ke || !nq) return;
+    if (!d_scores || !d_ids) fail(ORDVEC_STATUS_NULL_POINTER, "output pointer is NULL");
+    Workspace& w = workspace();
+    cudaStream_t st = (cudaStream_t)stream;
+    uint32_t got = 0;
+    int mode = 0;
+    switch (ix.kind) {
+      case ORDVEC_INDEX_KIND_RANK_QUANT:
+        got = asym ? engine_rankquant_full(ix, d_queries, nq, ke, w, st)
+                   : engine_rankquant_symmetric(ix, d_queries, nq, ke, w, st);
+        break;
+      case OVB_INDEX_KIND_RANK:
+        got = engine_rank_full(ix, d_queries, nq, ke, asym, w, st);
+        break;
+      case ORDVEC_INDEX_KIND_BITMAP:
+        got = engine_bitmap_full(ix, d_queries, nq, ke, w, st);
+        mode = 1;
+        break;
+      default:
+        got = engine_fastscan_full(ix, d_queries, nq, ke, w, st);
+    }
+    launch_keys_to_results(w.out_keys.as<uint32_t>(), w.out_ids.as<uint32_t>(), nq * got, mode, ix.n_top, d_scores,
+                           d_ids, st);
+  });
+}
+
 ordvec_status_t ovb_two_stage_profile(const ordvec_index_t* rq, const ordvec_index_t* stage1,
                                       const float* d_queries, uint64_t nq, uint64_t m, uint64_t k,
                                       float* d_scores, int64_t* d_ids, void* stream, float* stage_ms) {

@@ -259,13 +259,12 @@ static uint64_t split_filter_bytes_per_query(const FilterPlan& fp, uint64_t kp) 
 // result is then not known to be exact and the caller redoes the rows.
 // Kept sets are prefixes of the split-key order, so their top-kp is the
 // whole index's.
-static void split_filtered(const Index& rq, const uint16_t* qs, const float* qu, const float* l1, uint64_t qn, uint32_t ke,
-                    uint32_t kp, const FilterPlan& fp, uint32_t q_per_tile, uint32_t* d_flag, uint32_t* out_keys,
-                    uint32_t* out_ids, Workspace& w, cudaStream_t st) {
+static void split_filtered(const Index& rq, const uint16_t* qs, const float* qu, const float* l1, float inv_norm,
+                           uint64_t qn, uint32_t ke, uint32_t kp, const FilterPlan& fp, uint32_t q_per_tile,
+                           uint32_t* d_flag, uint32_t* out_keys, uint32_t* out_ids, Workspace& w, cudaStream_t st) {
   const uint64_t n = rq.n;
   const uint32_t dim = rq.dim, bits = rq.bits, id_bits = bits_for(n - 1);
   const uint8_t* codes = rq.codes.as<uint8_t>();
-  const float inv_norm = inv_rankquant_norm(dim, bits);
   uint32_t* err = w.tc_err_word(st);
   uint32_t* smp = (uint32_t*)w.smp_keys.ensure(qn * fp.n_s * 4);
   launch_rank_scan_tc(codes, n, dim, bits, qs, qn, inv_norm, fp.stride, smp, fp.n_s, q_per_tile, err, st);
@@ -296,17 +295,18 @@ static void split_filtered(const Index& rq, const uint16_t* qs, const float* qu,
   w.mark(st, 5);
 }
 
-uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t nq, uint64_t k, bool exact,
-                                     Workspace& w, cudaStream_t st, uint32_t q_per_tile) {
-  require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "search_asymmetric");
+// Split-BF16 search of prepared query rows qu (nq x dim f32) scored as
+// sum_j qu[j] (code_j - c) * inv_norm: the unit query and 1/norm for
+// search_asymmetric, the centred query buckets and 1/norm^2 for the symmetric
+// search.  The error bound is linear in |qu|_1 and inv_norm, so both share it.
+static uint32_t split_search(const Index& rq, const float* qu, float inv_norm, uint64_t nq, uint64_t k, bool exact,
+                             Workspace& w, cudaStream_t st, uint32_t q_per_tile) {
   if (!rank_tc_eligible(rq.dim, rq.bits))
     fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "split-BF16 scan needs dim to be a multiple of 64");
   const uint64_t n = rq.n;
   const uint32_t ke = (uint32_t)(k < n ? k : n);
   if (!ke || !nq) return ke;
   const uint32_t dim = rq.dim, bits = rq.bits;
-  const float* qu = normalised(w, d_q, nq, dim, st);
-  const float inv_norm = inv_rankquant_norm(dim, bits);
   const float bound = split_error_bound(dim, bits, inv_norm);
   uint16_t* qs = (uint16_t*)w.q_split.ensure(nq * 2 * dim * 2);
   float* l1 = (float*)w.q_l1.ensure(nq * 4);
@@ -328,8 +328,8 @@ uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t
     for (uint64_t q0 = 0; q0 < nq; q0 += fc) {
       const uint64_t qn = nq - q0 < fc ? nq - q0 : fc;
       OVB_CUDA(cudaMemsetAsync(flag, 0, 4, st));
-      split_filtered(rq, qs + q0 * 2 * dim, qu + q0 * dim, l1 + q0, qn, ke, (uint32_t)kp0, fp, q_per_tile, flag,
-                     ok + q0 * ke, oi + q0 * ke, w, st);
+      split_filtered(rq, qs + q0 * 2 * dim, qu + q0 * dim, l1 + q0, inv_norm, qn, ke, (uint32_t)kp0, fp, q_per_tile,
+                     flag, ok + q0 * ke, oi + q0 * ke, w, st);
       OVB_CUDA(cudaMemcpyAsync(flag_h, flag, 4, cudaMemcpyDeviceToHost, st));
       OVB_CUDA(cudaStreamSynchronize(st));
       if (!*flag_h) {
@@ -384,6 +384,17 @@ uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t
   return ke;
 }
 
+uint32_t engine_rankquant_full_split(const Index& rq, const float* d_q, uint64_t nq, uint64_t k, bool exact,
+                                     Workspace& w, cudaStream_t st, uint32_t q_per_tile) {
+  require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "search_asymmetric");
+  if (!rank_tc_eligible(rq.dim, rq.bits))
+    fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "split-BF16 scan needs dim to be a multiple of 64");
+  const uint64_t ke = k < rq.n ? k : rq.n;
+  if (!ke || !nq) return (uint32_t)ke;
+  const float* qu = normalised(w, d_q, nq, rq.dim, st);
+  return split_search(rq, qu, inv_rankquant_norm(rq.dim, rq.bits), nq, k, exact, w, st, q_per_tile);
+}
+
 bool split_fixed_fits(const Index& rq, uint64_t nq, uint64_t k) {
   const uint64_t n = rq.n, ke = k < n ? k : n;
   const uint64_t kp = std::min<uint64_t>(std::max<uint64_t>(2 * ke, ke + 64), n);
@@ -413,7 +424,7 @@ uint32_t engine_rankquant_split_fixed(const Index& rq, const float* d_q, uint64_
   uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
   uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
   if (filtered) {
-    split_filtered(rq, qs, qu, l1, nq, ke, (uint32_t)kp, fp, q_per_tile, d_flag, ok, oi, w, st);
+    split_filtered(rq, qs, qu, l1, inv_norm, nq, ke, (uint32_t)kp, fp, q_per_tile, d_flag, ok, oi, w, st);
     return ke;
   }
   uint32_t* keys = (uint32_t*)w.keys.ensure(nq * n * 4);
@@ -463,6 +474,9 @@ uint32_t engine_rankquant_symmetric(const Index& rq, const float* d_q, uint64_t 
   launch_encode(6, d_q, nq, rq.dim, rq.bits, 0, 0, qc, 0, st);
   const float norm = rankquant_norm_f32(rq.dim, rq.bits);
   const float inv_norm_sq = 1.0f / (norm * norm);
+  // batches: split-BF16 candidates (the centred buckets are exact in BF16, so
+  // lo = 0) rescored exactly
+  if (use_rank_tc(rq, nq)) return split_search(rq, qc, inv_norm_sq, nq, k, true, w, st, 0);
   uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
   uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
   full_scan_select(w, nq, rq.n, ke, 32, ok, oi, st, [&](uint64_t q0, uint64_t qn, uint32_t* keys) {

@@ -581,8 +581,10 @@ void launch_select_rows(const SelectArgs& a, uint64_t rows, uint64_t* scratch,
     launch_select_wide(a, rows, scratch, stream);
     return;
   }
-  // few long rows: one 8-CTA cluster per row
-  if (!a.row_off && !a.row_len && a.k <= kClusterCap && a.n >= 32768 && rows * kClusterCtas <= 2 * 148) {
+  // few long rows: one 8-CTA cluster per row (below two rows per SM the
+  // per-row form leaves SMs idle, and one CTA alone streams a long row slowly)
+  if (!a.row_off && !a.row_len && a.k <= kClusterCap && a.n >= 32768 &&
+      (rows * kClusterCtas <= 2 * 148 || (a.n >= (1ull << 18) && rows < 2 * 148))) {
     select_rows_cluster_kernel<<<(unsigned)(rows * kClusterCtas), kSelThreads, 0, stream>>>(a);
     launched();
     return;

@@ -35,7 +35,8 @@ def test_rank_encoder_matches_oracle(orc, dim):
     assert np.array_equal(rk.payload().view(np.uint16), orc.rank_encode(docs, dim))
 
 
-@pytest.mark.parametrize("dim,n,nq", [(64, 3000, 1), (100, 2500, 7), (768, 6000, 70), (1024, 20000, 3)])
+@pytest.mark.parametrize("dim,n,nq", [(64, 3000, 1), (100, 2500, 7), (200, 3000, 9), (768, 6000, 70),
+                                      (1024, 20000, 3), (2560, 2000, 5)])
 def test_rank_search_is_bit_exact(orc, dim, n, nq):
     docs = _docs(dim, n, 11 + dim)
     qs = _docs(dim, nq, 17 + dim)
@@ -143,3 +144,59 @@ def test_rank_ovr_fixture_bytes_and_roundtrip(tmp_path):
     qs = _docs(256, 4, 6)
     a, b = rk.search(qs, 25), back.search(qs, 25)
     assert np.array_equal(a.indices, b.indices) and np.array_equal(a.scores, b.scores)
+
+
+@pytest.mark.parametrize("bits", [1, 2, 4])
+def test_rankquant_symmetric_tensor_core_batches(orc, monkeypatch, bits):
+    """Batches of >= 64 queries take the split-BF16 scan (through the sampled
+    threshold filter at this size) with exact rescoring: the same bits as the
+    CUDA-core scan and the oracle, heavy score ties included."""
+    dim, n, nq = 768, 40000, 64
+    docs = _docs(dim, n, 41 + bits)
+    docs[100:400] = docs[7]  # 300 duplicate rows: ties across the k-th score
+    qs = _docs(dim, nq, 43)
+    qs[1] = docs[7]
+    rq = ob.RankQuant(dim, bits)
+    rq.add(docs)
+    packed = orc.rankquant_encode(docs, dim, bits)
+    for k in (10, 257):
+        monkeypatch.setenv("OVB_RANK_TC", "1")
+        tc = rq.search(qs, k)
+        monkeypatch.setenv("OVB_RANK_TC", "0")
+        plain = rq.search(qs, k)
+        assert np.array_equal(tc.indices, plain.indices), k
+        assert np.array_equal(tc.scores.view(np.uint32), plain.scores.view(np.uint32)), k
+        ws, wi = orc.rq_search_sym(packed, n, dim, bits, qs[:4], k)
+        assert np.array_equal(tc.indices.reshape(nq, -1)[:4], wi), k
+        assert np.array_equal(tc.scores.reshape(nq, -1)[:4].view(np.uint32), ws.view(np.uint32)), k
+
+
+def test_search_device_matches_host_entry_points():
+    """ovb_index_search_device gives the host entry points' results for every
+    kind with a full search, on the caller's stream."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    dim, n, nq, k = 256, 5000, 6, 17
+    docs = _docs(dim, n, 51)
+    qs = _docs(dim, nq, 52)
+    rq, rk, bm, fs = ob.RankQuant(dim, 2), ob.Rank(dim), ob.Bitmap(dim, 64), ob.RankQuantFastscan(dim)
+    for ix in (rq, rk, bm, fs):
+        ix.add(docs)
+    d_q = torch.from_numpy(qs).to(dev)
+    cases = [(rq, False, rq.search), (rq, True, rq.search_asymmetric), (rk, False, rk.search),
+             (rk, True, rk.search_asymmetric), (bm, False, bm.search), (fs, False, fs.search)]
+    for ix, asym, host in cases:
+        d_s = torch.empty(nq * k, dtype=torch.float32, device=dev)
+        d_i = torch.empty(nq * k, dtype=torch.int64, device=dev)
+        ob.search_device(ix, d_q.data_ptr(), nq, k, d_s.data_ptr(), d_i.data_ptr(), stream.cuda_stream,
+                         asymmetric=asym)
+        torch.cuda.synchronize(dev)
+        want = host(qs, k)
+        name = type(ix).__name__
+        assert np.array_equal(d_i.cpu().numpy(), want.indices), (name, asym)
+        assert np.array_equal(d_s.cpu().numpy().view(np.uint32), want.scores.view(np.uint32)), (name, asym)
+    with pytest.raises(OrdvecError) as e:
+        ob.search_device(bm, d_q.data_ptr(), nq, k, 0, 0, stream.cuda_stream, asymmetric=True)
+    assert e.value.status == 11
