@@ -471,6 +471,8 @@ def profile_case(case: str):
       popc      the same index, one query per call (popc_rows_kernel, wide select)
       rank      RankQuant(1024, 2) exact top-100 of 1024 queries, N=1M (rank_tc_kernel)
       fastscan  this workload's FastScan top-1000 of 1000 queries (fastscan_tc_kernel)
+      plain     this workload's two-stage search, one query per call, 12 calls
+                (fastscan_scan_kernel, select_rows_cluster_kernel, rerank)
       rankfull  Rank(768) N=1M top-100: symmetric then asymmetric, 1 query and 64
                 queries per call (rank_tile_kernel)
     Each search runs more than once so captures can skip the first call."""
@@ -497,6 +499,14 @@ def profile_case(case: str):
         q, _ = ob.synth_queries(SEED + 1, N_DOCS, NQ, DIM)
         for _ in range(2):
             fs.search(q, M)
+    elif case == "plain":
+        rq, fs = ob.RankQuant(DIM, 2), ob.RankQuantFastscan(DIM)
+        docs = ob.synth_docs(SEED, N_DOCS, DIM)
+        rq.add(docs)
+        fs.add(docs)
+        q, _ = ob.synth_queries(SEED + 1, N_DOCS, 12, DIM)
+        for i in range(12):
+            ob.two_stage_search(rq, fs, q[i:i + 1], M, K)
     elif case == "rankfull":
         n = 1_000_000
         rk = ob.Rank(768)
@@ -627,7 +637,7 @@ def main():
                          "0 = skip, -1 = 4096 on a single GPU")
     ap.add_argument("--large", default="auto", choices=["auto", "on", "off"],
                     help="also run the N=10M dim-768 bitmap / multi-bucket configuration (auto: one GPU only)")
-    ap.add_argument("--profile-case", choices=["bitmap", "popc", "rank", "fastscan", "rankfull"],
+    ap.add_argument("--profile-case", choices=["bitmap", "popc", "rank", "fastscan", "plain", "rankfull"],
                     help="run one small kernel workload for an ncu capture and exit")
     args = ap.parse_args()
     if args.profile_case:

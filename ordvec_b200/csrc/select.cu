@@ -189,12 +189,16 @@ __global__ void __launch_bounds__(kSelThreads)
 // the per-CTA histograms are summed through distributed shared memory, every
 // CTA derives the same bin, and the winners are gathered into CTA 0's shared
 // memory, which sorts and writes them.  All waits are hardware cluster
-// barriers.
+// barriers.  When a CTA's slice fits (stage != 0), the first pass also copies
+// the slice's keys (and explicit ids) into dynamic shared memory and the later
+// passes read them there: the passes are otherwise bound by the latency of
+// re-reading the slice from L2.
 constexpr int kClusterCtas = 8;
 constexpr uint32_t kClusterCap = 2048;
+constexpr uint64_t kClusterStageBytes = 160 * 1024;
 
 __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kSelThreads)
-    select_rows_cluster_kernel(SelectArgs a) {
+    select_rows_cluster_kernel(SelectArgs a, uint32_t stage) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   __shared__ uint32_t hist[kHistBins];
@@ -219,6 +223,23 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kSelThrea
   const uint64_t per = (n + kClusterCtas - 1) / kClusterCtas;
   const uint64_t lo = crank * per < n ? crank * per : n;
   const uint64_t hi = lo + per < n ? lo + per : n;
+  extern __shared__ __align__(16) uint32_t st_keys[];  // [per] keys, then [per] ids when explicit
+  uint32_t* st_ids = st_keys + per;
+  // key i of this CTA's slice; pass 0 fills the stage
+  auto key_at = [&](uint64_t i, bool first) -> uint64_t {
+    if (!stage) return load_key(keys, ids, i);
+    uint32_t k32, id;
+    if (first) {
+      k32 = keys[i];
+      st_keys[i - lo] = k32;
+      id = ids ? ids[i] : (uint32_t)i;
+      if (ids) st_ids[i - lo] = id;
+    } else {
+      k32 = st_keys[i - lo];
+      id = ids ? st_ids[i - lo] : (uint32_t)i;
+    }
+    return ((uint64_t)k32 << 32) | id;
+  };
 
   Digit digits[8];
   int nd = 0;
@@ -242,7 +263,7 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kSelThrea
     for (uint32_t b = threadIdx.x; b < kHistBins; b += blockDim.x) hist[b] = 0;
     cluster.sync();
     for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-      uint64_t key = load_key(keys, ids, i);
+      uint64_t key = key_at(i, d == 0);
       if ((key & fixed) == prefix) atomicAdd(&hist[(uint32_t)(key >> shift) & (nbins - 1)], 1u);
     }
     cluster.sync();
@@ -310,8 +331,10 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kSelThrea
   uint32_t* below0 = cluster.map_shared_rank(&s_cnt_below, 0);
   uint32_t* tie0 = cluster.map_shared_rank(&s_cnt_tie, 0);
   if (k_eff > 0) {
+    // the stage was filled only if some digit pass ran
+    const bool first = nd == 0 || k_eff == n;
     for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-      uint64_t key = load_key(keys, ids, i);
+      uint64_t key = key_at(i, first);
       uint64_t m = key & fixed;
       if (m < prefix) {
         uint32_t slot = atomicAdd(below0, 1u);
@@ -585,7 +608,14 @@ void launch_select_rows(const SelectArgs& a, uint64_t rows, uint64_t* scratch,
   // per-row form leaves SMs idle, and one CTA alone streams a long row slowly)
   if (!a.row_off && !a.row_len && a.k <= kClusterCap && a.n >= 32768 &&
       (rows * kClusterCtas <= 2 * 148 || (a.n >= (1ull << 18) && rows < 2 * 148))) {
-    select_rows_cluster_kernel<<<(unsigned)(rows * kClusterCtas), kSelThreads, 0, stream>>>(a);
+    const uint64_t per = (a.n + kClusterCtas - 1) / kClusterCtas;
+    const uint64_t bytes = per * (a.ids ? 8 : 4);
+    const uint32_t stage = bytes <= kClusterStageBytes ? 1u : 0u;
+    const size_t smem = stage ? (size_t)bytes : 0;
+    if (smem > 48 * 1024)
+      OVB_CUDA(cudaFuncSetAttribute(select_rows_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+    select_rows_cluster_kernel<<<(unsigned)(rows * kClusterCtas), kSelThreads, smem, stream>>>(a, stage);
     launched();
     return;
   }
