@@ -198,6 +198,17 @@ ordvec_status_t ovb_rankquant_search_split(const ordvec_index_t *rq, const float
  * Bitmap; RankQuantFastscan), OVB_SEARCH_ASYMMETRIC its `search_asymmetric`
  * (RankQuant, Rank).  Calls from one thread share its workspace and must be
  * ordered on one stream. */
+/* Failure-path self-tests (no counterpart in the reference).  The tensor-core
+ * kernels bound every mbarrier wait (about 1 s); a wait that gives up sets the
+ * calling thread's error word, drains, frees its TMEM and returns, and the host
+ * entry point then fails with ORDVEC_STATUS_INTERNAL.
+ * ovb_selftest_bounded_wait runs that bounded wait on a barrier nothing
+ * arrives at: *timed_out = 1 and *waited_ns its duration.
+ * ovb_selftest_arm_tc_error sets the calling thread's error word, so that its
+ * next search that runs a tensor-core kernel reports INTERNAL (and re-arms). */
+ordvec_status_t ovb_selftest_bounded_wait(uint32_t *timed_out, uint64_t *waited_ns);
+ordvec_status_t ovb_selftest_arm_tc_error(void);
+
 #define OVB_SEARCH_DEFAULT 0u
 #define OVB_SEARCH_ASYMMETRIC 1u
 ordvec_status_t ovb_index_search_device(const ordvec_index_t *index, uint32_t method, const float *d_queries,

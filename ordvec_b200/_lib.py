@@ -121,6 +121,8 @@ SIGNATURES = {
     "ovb_rankquant_search_symmetric": (S, [P, P, U64, U64, P, P]),
     "ovb_rank_search": (S, [P, P, U64, U64, P, P]),
     "ovb_index_search_device": (S, [P, U32, P, U64, U64, P, P, P]),
+    "ovb_selftest_bounded_wait": (S, [P, P]),
+    "ovb_selftest_arm_tc_error": (S, []),
     "ovb_rank_search_asymmetric": (S, [P, P, U64, U64, P, P]),
     "ovb_rankquant_search_mixed": (S, [P, U32, P, P, P, U64, U64, P, P]),
     "ovb_mixed_plan_info": (S, [P, U64, U64, P, P, P]),

@@ -171,8 +171,18 @@ void download_results(Workspace& w, uint64_t count, int mode, uint32_t n_top, fl
   launch_keys_to_results(w.out_keys.as<uint32_t>(), w.out_ids.as<uint32_t>(), count, mode, n_top, ds, di, w.stream);
   OVB_CUDA(cudaMemcpyAsync(scores, ds, count * 4, cudaMemcpyDeviceToHost, w.stream));
   OVB_CUDA(cudaMemcpyAsync(ids, di, count * 8, cudaMemcpyDeviceToHost, w.stream));
+  // the tensor-core error word comes back with the results: one synchronisation
+  uint32_t* h_err = w.tc_used ? (uint32_t*)w.pinned.ensure(4) : nullptr;
+  if (h_err) OVB_CUDA(cudaMemcpyAsync(h_err, w.tc_err.p, 4, cudaMemcpyDeviceToHost, w.stream));
   OVB_CUDA(cudaStreamSynchronize(w.stream));
-  check_tc(w);
+  if (h_err) {
+    w.tc_used = false;
+    if (*h_err) {
+      OVB_CUDA(cudaMemsetAsync(w.tc_err.p, 0, 4, w.stream));
+      OVB_CUDA(cudaStreamSynchronize(w.stream));
+      fail(ORDVEC_STATUS_INTERNAL, "tensor-core FastScan scan: a bounded wait timed out; results discarded");
+    }
+  }
 }
 
 void need_queries(const float* q, uint64_t nq) {
@@ -839,6 +849,30 @@ ordvec_status_t ovb_two_stage_search_device(const ordvec_index_t* rq, const ordv
     cudaStream_t st = (cudaStream_t)stream;
     uint32_t got = engine_two_stage(r, s, d_queries, nq, m, k, w, st);
     launch_keys_to_results(w.out_keys.as<uint32_t>(), w.out_ids.as<uint32_t>(), nq * got, 0, 0, d_scores, d_ids, st);
+  });
+}
+
+ordvec_status_t ovb_selftest_bounded_wait(uint32_t* timed_out, uint64_t* waited_ns) {
+  return boundary([&] {
+    if (!timed_out || !waited_ns) fail(ORDVEC_STATUS_NULL_POINTER, "output pointer is NULL");
+    Workspace& w = workspace();
+    uint32_t* d = (uint32_t*)w.flag.ensure(16);
+    uint32_t* h = (uint32_t*)w.pinned.ensure(16);
+    launch_wait_probe(d, w.stream);
+    OVB_CUDA(cudaMemcpyAsync(h, d, 12, cudaMemcpyDeviceToHost, w.stream));
+    OVB_CUDA(cudaStreamSynchronize(w.stream));
+    *timed_out = h[0];
+    *waited_ns = (uint64_t)h[1] | ((uint64_t)h[2] << 32);
+  });
+}
+
+ordvec_status_t ovb_selftest_arm_tc_error(void) {
+  return boundary([&] {
+    Workspace& w = workspace();
+    uint32_t* e = w.tc_err_word(w.stream);
+    w.tc_used = false;  // only armed: the next search that runs a tensor-core kernel reads it
+    OVB_CUDA(cudaMemsetAsync(e, 0x01, 4, w.stream));
+    OVB_CUDA(cudaStreamSynchronize(w.stream));
   });
 }
 

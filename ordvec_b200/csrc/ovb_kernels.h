@@ -131,6 +131,10 @@ void launch_rank_filter_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint3
 void launch_split_margin(const uint32_t* sel_keys, uint64_t nq, uint32_t kp, uint32_t k, const float* l1,
                          float bound_per_l1, uint32_t* flag, cudaStream_t stream);
 
+// ---- self-test (selftest.cu): out[0] = 1 when a bounded mbarrier wait on a
+// barrier nothing arrives at gave up, out[1..2] = the nanoseconds it waited
+void launch_wait_probe(uint32_t* d_out, cudaStream_t stream);
+
 // ---- K9 Rank (u16) index scans (scan_rank_full.cu) -> key32 [nq][ld] ------------
 float rank_norm_f32(uint32_t dim);
 // Rank::search: q_ranks = the queries' u16 ranks (nq x dim)
