@@ -99,6 +99,17 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ CPU baseline
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_two_stage_qps(docs, queries, budget_s: float):
     """Time the oracle's AVX-512/OpenMP restatement on a bounded query sample."""
     from oracle import oracle as orc
@@ -114,7 +125,12 @@ def cpu_two_stage_qps(docs, queries, budget_s: float):
     t0 = time.perf_counter()
     s, i = orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[:sample], M, K, threads)
     dt = time.perf_counter() - t0
-    return sample / dt, threads, sample, (s, i), blocks, packed
+    # one thread, a small sample (about a second)
+    one = min(len(queries), 16)
+    t1 = time.perf_counter()
+    orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[:one], M, K, 1)
+    qps1 = one / (time.perf_counter() - t1)
+    return sample / dt, threads, sample, (s, i), blocks, packed, qps1
 
 
 def reference_arm(args):
@@ -816,9 +832,11 @@ def main():
         "clocks": clock_info,
     }
     if rank == 0 and not args.no_cpu:
-        qps, threads, sample, _, _, _ = cpu_two_stage_qps(docs, queries, args.cpu_seconds)
+        qps, threads, sample, _, _, _, qps1 = cpu_two_stage_qps(docs, queries, args.cpu_seconds)
         line["cpu_baseline"] = {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
-                                "sample": f"first {sample} of the step's {NQ} queries, all host threads"}
+                                "sample": f"first {sample} of the step's {NQ} queries, all host threads",
+                                "value_1thread": qps1, "sample_1thread": "first 16 queries, one thread",
+                                "cpu_model": cpu_model()}
     group.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
