@@ -133,10 +133,20 @@ Index* new_index(uint32_t kind, uint32_t dim, uint32_t bits, uint32_t n_top) {
   return ix;
 }
 
+// Up to this many values the finiteness check runs on the host while the copy
+// is in flight (a few microseconds, no device round trip); larger batches are
+// checked by a kernel, faster than one host thread.
+constexpr uint64_t kHostFiniteMax = 1u << 16;
+
 const float* upload_queries(Workspace& w, const float* q, uint64_t nq, uint32_t dim, bool check) {
   float* d = (float*)w.q_raw.ensure(nq * dim * 4);
   OVB_CUDA(cudaMemcpyAsync(d, q, nq * dim * 4, cudaMemcpyHostToDevice, w.stream));
-  if (check) {
+  if (check && nq * dim <= kHostFiniteMax) {
+    if (!all_finite(q, nq * dim)) {
+      OVB_CUDA(cudaStreamSynchronize(w.stream));  // the copy still reads the caller's buffer
+      fail(ORDVEC_STATUS_NONFINITE_QUERY, "query contains NaN or infinity");
+    }
+  } else if (check) {
     uint32_t* flag = (uint32_t*)w.flag.ensure(4);
     uint32_t* h = (uint32_t*)w.pinned.ensure(4);
     OVB_CUDA(cudaMemsetAsync(flag, 0, 4, w.stream));

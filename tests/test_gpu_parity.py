@@ -396,6 +396,13 @@ def test_nonfinite_queries_are_rejected(corpus):
     with pytest.raises(ob.OrdvecError) as e:
         rq.search_asymmetric(bad, 5)
     assert e.value.status == 8
+    # a batch above the host-checked size takes the device check
+    big = np.tile(queries, (16, 1))
+    big[100, 7] = np.nan
+    with pytest.raises(ob.OrdvecError) as e:
+        rq.search_asymmetric(big, 5)
+    assert e.value.status == 8
+    assert rq.search_asymmetric(big[:64], 5).k == 5
 
 
 # ---------------------------------------------------------------- FastScan
