@@ -189,10 +189,10 @@ __global__ void __launch_bounds__(kSelThreads)
 // the per-CTA histograms are summed through distributed shared memory, every
 // CTA derives the same bin, and the winners are gathered into CTA 0's shared
 // memory, which sorts and writes them.  All waits are hardware cluster
-// barriers.  When a CTA's slice fits (stage != 0), the first pass also copies
-// the slice's keys (and explicit ids) into dynamic shared memory and the later
-// passes read them there: the passes are otherwise bound by the latency of
-// re-reading the slice from L2.
+// barriers.  When a CTA's slice fits (stage != 0) it is first copied into
+// dynamic shared memory (keys, and explicit ids) with several loads in flight
+// per thread, and every pass reads it there: the passes are otherwise bound by
+// the latency of re-reading the slice from L2.
 constexpr int kClusterCtas = 8;
 constexpr uint32_t kClusterCap = 2048;
 constexpr uint64_t kClusterStageBytes = 160 * 1024;
@@ -205,7 +205,7 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kSelThrea
   __shared__ uint32_t tot[kHistBins];
   __shared__ uint32_t warp_tot[kSelThreads / 32];
   __shared__ uint64_t sbuf[kClusterCap];
-  __shared__ uint32_t s_bin, s_before, s_in_bin, s_cnt_below, s_cnt_tie;
+  __shared__ uint32_t s_bin, s_before, s_in_bin, s_cnt_below, s_cnt_tie, s_ctie;
 
   const uint32_t crank = cluster.block_rank();
   const uint64_t row = blockIdx.x / kClusterCtas;
@@ -225,25 +225,41 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kSelThrea
   const uint64_t hi = lo + per < n ? lo + per : n;
   extern __shared__ __align__(16) uint32_t st_keys[];  // [per] keys, then [per] ids when explicit
   uint32_t* st_ids = st_keys + per;
-  // key i of this CTA's slice; pass 0 fills the stage
-  auto key_at = [&](uint64_t i, bool first) -> uint64_t {
-    if (!stage) return load_key(keys, ids, i);
-    uint32_t k32, id;
-    if (first) {
-      k32 = keys[i];
-      st_keys[i - lo] = k32;
-      id = ids ? ids[i] : (uint32_t)i;
-      if (ids) st_ids[i - lo] = id;
-    } else {
-      k32 = st_keys[i - lo];
-      id = ids ? st_ids[i - lo] : (uint32_t)i;
+  // Stage the slice once, eight loads in flight per thread (one pass of
+  // dependent loads would wait out the memory latency once per key).
+  if (stage) {
+    for (uint64_t i0 = lo + threadIdx.x; i0 < hi; i0 += 8ull * blockDim.x) {
+      uint32_t v[8], u[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint64_t i = i0 + (uint64_t)j * blockDim.x;
+        v[j] = i < hi ? keys[i] : 0u;
+        u[j] = i < hi && ids ? ids[i] : 0u;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint64_t i = i0 + (uint64_t)j * blockDim.x;
+        if (i < hi) {
+          st_keys[i - lo] = v[j];
+          if (ids) st_ids[i - lo] = u[j];
+        }
+      }
     }
-    return ((uint64_t)k32 << 32) | id;
+    __syncthreads();
+  }
+  // key i of this CTA's slice
+  auto key_at = [&](uint64_t i) -> uint64_t {
+    if (!stage) return load_key(keys, ids, i);
+    return ((uint64_t)st_keys[i - lo] << 32) | (ids ? st_ids[i - lo] : (uint32_t)i);
   };
 
+  // Digits of key32 and, for explicit ids, of the id.  When the id is the
+  // position (ids == null), ties left after the key digits are resolved by
+  // position instead: the CTAs' slices are ordered, so the lowest positions are
+  // the first CTAs' ties in slice order (two passes fewer).
   Digit digits[8];
   int nd = 0;
-  for (int part = 0; part < 2; part++) {
+  for (int part = 0; part < (ids ? 2 : 1); part++) {
     uint32_t bits = part == 0 ? a.key_bits : a.id_bits;
     uint32_t top = (part == 0 ? 32u : 0u) + bits;
     while (bits > 0) {
@@ -262,9 +278,17 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kSelThrea
     const uint32_t nbins = 1u << width;
     for (uint32_t b = threadIdx.x; b < kHistBins; b += blockDim.x) hist[b] = 0;
     cluster.sync();
-    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-      uint64_t key = key_at(i, d == 0);
-      if ((key & fixed) == prefix) atomicAdd(&hist[(uint32_t)(key >> shift) & (nbins - 1)], 1u);
+    for (uint64_t i0 = lo + threadIdx.x; i0 < hi; i0 += 4ull * blockDim.x) {  // four keys in flight
+      uint64_t kk[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const uint64_t i = i0 + (uint64_t)j * blockDim.x;
+        kk[j] = i < hi ? key_at(i) : 0;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (i0 + (uint64_t)j * blockDim.x < hi && (kk[j] & fixed) == prefix)
+          atomicAdd(&hist[(uint32_t)(kk[j] >> shift) & (nbins - 1)], 1u);
     }
     cluster.sync();
     for (uint32_t b = threadIdx.x; b < kHistBins; b += blockDim.x) {
@@ -330,19 +354,55 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kSelThrea
   uint64_t* buf0 = cluster.map_shared_rank(sbuf, 0);
   uint32_t* below0 = cluster.map_shared_rank(&s_cnt_below, 0);
   uint32_t* tie0 = cluster.map_shared_rank(&s_cnt_tie, 0);
+  // more ties than needed and ids are positions: take the lowest positions
+  const bool by_pos = !ids && !take_all && k_eff > 0;
   if (k_eff > 0) {
-    // the stage was filled only if some digit pass ran
-    const bool first = nd == 0 || k_eff == n;
     for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-      uint64_t key = key_at(i, first);
+      uint64_t key = key_at(i);
       uint64_t m = key & fixed;
       if (m < prefix) {
         uint32_t slot = atomicAdd(below0, 1u);
         if (slot < below_total) buf0[slot] = key;
-      } else if (m == prefix) {
+      } else if (m == prefix && !by_pos) {
         uint32_t tk = atomicAdd(tie0, 1u);
         if (tk < need) buf0[below_total + tk] = key;
       }
+    }
+  }
+  if (by_pos) {
+    // each thread owns a contiguous run of the slice: count its ties, scan the
+    // counts over the CTA, add the ties of the lower-ranked CTAs, then write
+    // the ties whose rank falls below `need` at that rank
+    const uint64_t run = (hi - lo + blockDim.x - 1) / blockDim.x;
+    const uint64_t r0 = lo + threadIdx.x * run < hi ? lo + threadIdx.x * run : hi;
+    const uint64_t r1 = r0 + run < hi ? r0 + run : hi;
+    uint32_t mine = 0;
+    for (uint64_t i = r0; i < r1; i++) mine += (key_at(i) & fixed) == prefix ? 1u : 0u;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      const uint32_t v = warp_tot[lane];
+      uint32_t x = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+      }
+      warp_tot[lane] = x - v;
+      if (lane == 31) s_ctie = x;
+    }
+    __syncthreads();
+    uint32_t rank = warp_tot[w] + incl - mine;
+    cluster.sync();  // every CTA's s_ctie is set
+    for (uint32_t r = 0; r < crank; r++) rank += *cluster.map_shared_rank(&s_ctie, r);
+    for (uint64_t i = r0; i < r1 && rank < need; i++) {
+      const uint64_t key = key_at(i);
+      if ((key & fixed) == prefix) buf0[below_total + rank++] = key;
     }
   }
   cluster.sync();

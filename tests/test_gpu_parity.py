@@ -894,3 +894,27 @@ def test_persistence_roundtrip_all_formats(tmp_path, corpus):
     a = fs.search(queries, 20)
     b = ob.load(str(tmp_path / "x.ovfs")).search(queries, 20)
     assert np.array_equal(a.indices, b.indices)
+
+
+@pytest.mark.parametrize("nq", [1, 3, 20])
+def test_cluster_select_ties_by_position(orc, monkeypatch, nq):
+    """Long rows (>= 32,768 keys) of a few queries go through the 8-CTA cluster
+    select; with ids = positions its ties are taken lowest position first.
+    Bitmap overlaps tie massively (a few dozen distinct values over 100k docs),
+    and duplicate rows add exact ties across the CTAs' slices."""
+    monkeypatch.setenv("OVB_BITMAP_TC", "0")  # CUDA-core scan: the key matrix and the select
+    monkeypatch.setenv("OVB_SELECT_WIDE", "0")
+    dim, n_top, n = 256, 64, 100_003
+    rng = np.random.default_rng(77)
+    docs = rng.standard_normal((n, dim)).astype(np.float32)
+    docs[50_000:50_300] = docs[3]  # duplicates spread over two CTA slices
+    qs = rng.standard_normal((nq, dim)).astype(np.float32)
+    qs[0] = docs[3]
+    bm = ob.Bitmap(dim, n_top)
+    bm.add(docs)
+    words = orc.bitmap_encode(docs, dim, n_top)
+    for m in (1, 257, 1000, 2048):
+        got = bm.top_m_candidates_batched(qs, m)
+        for qi in range(nq):
+            want = orc.bitmap_top_m(words, n, dim, n_top, qs[qi], m)
+            assert np.array_equal(np.asarray(got[qi]), want), (m, qi)
