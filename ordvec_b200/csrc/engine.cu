@@ -36,8 +36,8 @@ float inv_rankquant_norm(uint32_t dim, uint32_t bits) { return 1.0f / rankquant_
 void select_rows(Workspace& w, const uint32_t* keys, const uint32_t* ids, const uint64_t* row_off,
                  uint64_t ld, uint64_t n, uint64_t rows, uint32_t k, uint32_t key_bits,
                  uint32_t id_bits, uint32_t* out_keys, uint32_t* out_ids, cudaStream_t st,
-                 const uint32_t* row_len = nullptr) {
-  SelectArgs a{keys, ids, row_off, ld, n, k, key_bits, id_bits, out_keys, out_ids, row_len};
+                 const uint32_t* row_len = nullptr, bool ordered = true) {
+  SelectArgs a{keys, ids, row_off, ld, n, k, key_bits, id_bits, out_keys, out_ids, row_len, ordered ? 0u : 1u};
   size_t se = select_rows_scratch_elems(rows, k, row_off ? 0 : n);
   uint64_t* scratch = se ? (uint64_t*)w.scratch.ensure(se * 8) : nullptr;
   launch_select_rows(a, rows, scratch, st);
@@ -58,7 +58,7 @@ void full_scan_select(Workspace& w, uint64_t nq, uint64_t n, uint32_t k, uint32_
     scan(q0, qn, keys);
     w.mark(st, 2);
     select_rows(w, keys, nullptr, nullptr, n, n, qn, k, key_bits, id_bits, out_keys + q0 * k,
-                out_ids + q0 * k, st);
+                out_ids + q0 * k, st, nullptr, !w.cand_unordered);
     w.mark(st, 3);
   }
 }
@@ -158,7 +158,7 @@ void filtered_select(Workspace& w, uint64_t n, uint64_t nq, uint32_t me, const F
     }
     w.mark(st, 2);
     select_rows(w, fk, fi, nullptr, fp.cap, fp.cap, qn, me, key_bits, bits_for(n - 1), sk + q0 * me, si + q0 * me,
-                st, cnt);
+                st, cnt, !w.cand_unordered);
     w.mark(st, 3);
   }
 }
@@ -671,7 +671,17 @@ uint32_t engine_two_stage(const Index& rq, const Index& s1, const float* d_q, ui
   w.mark(st, 0);
   if (!nq) return 0;
   const float* qu = normalised(w, d_q, nq, rq.dim, st);  // shared by both stages
-  const uint32_t me = engine_candidates(s1, d_q, nq, m_req, nullptr, w, st, qu);
+  // the rerank reads the candidate set, not its order: stage 1 skips the sort
+  struct Unordered {
+    Workspace& w;
+    explicit Unordered(Workspace& ws) : w(ws) { w.cand_unordered = true; }
+    ~Unordered() { w.cand_unordered = false; }
+  };
+  uint32_t me;
+  {
+    Unordered guard(w);
+    me = engine_candidates(s1, d_q, nq, m_req, nullptr, w, st, qu);
+  }
   const uint32_t ke = (uint32_t)(k < me ? k : me);
   if (!ke) return ke;
   uint64_t* off = (uint64_t*)w.off.ensure((nq + 1) * 8);

@@ -103,6 +103,7 @@ struct Workspace {
   // split-BF16 rank scan: [hi; lo] query rows and |q|_1
   DevBuf q_split, q_l1;
   uint64_t split_kp = 0;  // largest candidate count the last exact split search settled on
+  bool cand_unordered = false;  // set while a two-stage search selects its stage-1 set
   HostBuf pinned, f_flag_host;
   // error word of the tensor-core kernels (zeroed once; checked by host APIs)
   DevBuf tc_err;

@@ -23,6 +23,7 @@ struct SelectArgs {
   uint32_t* out_keys;
   uint32_t* out_ids;
   const uint32_t* row_len;  // optional: row r holds min(row_len[r], n) entries at r*ld
+  uint32_t unordered;       // 1: a row's k_eff winners in any order (the set only; per-row and cluster forms)
 };
 // u64 scratch elements launch_select_rows may use for `rows` rows of length n
 // (0 for ragged rows): global sort buffers for k > kSelectSmemCap, and the

@@ -172,11 +172,13 @@ __global__ void __launch_bounds__(kSelThreads)
     }
   }
   __syncthreads();
-  uint32_t len = 1;
-  while (len < k_eff) len <<= 1;
-  for (uint32_t j = k_eff + threadIdx.x; j < len; j += blockDim.x) buf[j] = ~0ull;
-  __syncthreads();
-  bitonic_sort(buf, len);
+  if (!a.unordered) {  // a caller that needs only the set skips the sort
+    uint32_t len = 1;
+    while (len < k_eff) len <<= 1;
+    for (uint32_t j = k_eff + threadIdx.x; j < len; j += blockDim.x) buf[j] = ~0ull;
+    __syncthreads();
+    bitonic_sort(buf, len);
+  }
   for (uint32_t j = threadIdx.x; j < k_eff; j += blockDim.x) {
     uint64_t key = buf[j];
     out_k[j] = (uint32_t)(key >> 32);
@@ -407,11 +409,13 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kSelThrea
   }
   cluster.sync();
   if (crank == 0 && k_eff > 0) {
-    uint32_t len = 1;
-    while (len < k_eff) len <<= 1;
-    for (uint32_t j = k_eff + threadIdx.x; j < len; j += blockDim.x) sbuf[j] = ~0ull;
-    __syncthreads();
-    bitonic_sort(sbuf, len);
+    if (!a.unordered) {
+      uint32_t len = 1;
+      while (len < k_eff) len <<= 1;
+      for (uint32_t j = k_eff + threadIdx.x; j < len; j += blockDim.x) sbuf[j] = ~0ull;
+      __syncthreads();
+      bitonic_sort(sbuf, len);
+    }
     for (uint32_t j = threadIdx.x; j < k_eff; j += blockDim.x) {
       out_k[j] = (uint32_t)(sbuf[j] >> 32);
       out_i[j] = (uint32_t)sbuf[j];
