@@ -24,6 +24,8 @@ namespace {
 
 constexpr int kSelThreads = 1024;
 constexpr int kHistBins = 2048;
+constexpr uint64_t kShortRow = 16384;  // rows up to this many keys take the 256-thread form
+constexpr uint32_t kShortCap = 2048;   // ... when k is at most this
 
 struct Digit {
   uint32_t shift, width;
@@ -55,11 +57,15 @@ __device__ void bitonic_sort(uint64_t* buf, uint32_t len) {
   }
 }
 
-__global__ void __launch_bounds__(kSelThreads)
+// T threads per row (1024; 256 for rows of at most kShortRow keys, so that
+// several rows share an SM), CAP sorted entries in shared memory.
+template <int T, uint32_t CAP>
+__global__ void __launch_bounds__(T)
     select_rows_kernel(SelectArgs a, uint64_t* gbuf, uint32_t gbuf_stride) {
+  constexpr int BPT = kHistBins / T;  // histogram bins per thread in the scan
   __shared__ uint32_t hist[kHistBins];
-  __shared__ uint32_t warp_tot[kSelThreads / 32];
-  __shared__ uint64_t sbuf[kSelectSmemCap];
+  __shared__ uint32_t warp_tot[T / 32];
+  __shared__ uint64_t sbuf[CAP];
   __shared__ uint32_t s_bin, s_before, s_in_bin, s_cnt_below, s_cnt_tie;
 
   const uint64_t row = blockIdx.x;
@@ -84,7 +90,7 @@ __global__ void __launch_bounds__(kSelThreads)
   }
   if (k_eff == 0) return;
 
-  uint64_t* buf = (k_eff <= kSelectSmemCap) ? sbuf : gbuf + row * (uint64_t)gbuf_stride;
+  uint64_t* buf = (k_eff <= CAP) ? sbuf : gbuf + row * (uint64_t)gbuf_stride;
 
   // digit schedule: key32 bits [32+key_bits-1, 32], then id bits [id_bits-1, 0]
   Digit digits[8];
@@ -113,10 +119,17 @@ __global__ void __launch_bounds__(kSelThreads)
       if ((key & fixed) == prefix) atomicAdd(&hist[(uint32_t)(key >> shift) & (nbins - 1)], 1u);
     }
     __syncthreads();
-    // block scan over bins (2 per thread) to find the bin holding the need-th key
+    // block scan over bins (BPT consecutive bins per thread) to find the bin
+    // holding the need-th key
     const uint32_t t = threadIdx.x;
-    uint32_t h0 = hist[2 * t], h1 = hist[2 * t + 1];
-    uint32_t s = h0 + h1, incl = s;
+    uint32_t hv[BPT];
+    uint32_t s = 0;
+#pragma unroll
+    for (int b = 0; b < BPT; b++) {
+      hv[b] = hist[BPT * t + b];
+      s += hv[b];
+    }
+    uint32_t incl = s;
     const int lane = t & 31, w = t >> 5;
     for (int o = 1; o < 32; o <<= 1) {
       uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
@@ -125,24 +138,26 @@ __global__ void __launch_bounds__(kSelThreads)
     if (lane == 31) warp_tot[w] = incl;
     __syncthreads();
     if (w == 0) {
-      uint32_t v = warp_tot[lane], x = v;
+      uint32_t v = lane < T / 32 ? warp_tot[lane] : 0u, x = v;
       for (int o = 1; o < 32; o <<= 1) {
         uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
         if (lane >= o) x += y;
       }
-      warp_tot[lane] = x - v;  // exclusive warp offsets
+      if (lane < T / 32) warp_tot[lane] = x - v;  // exclusive warp offsets
     }
     __syncthreads();
-    uint32_t excl = warp_tot[w] + incl - s;
+    const uint32_t excl = warp_tot[w] + incl - s;
     if (excl < need && need <= excl + s) {
-      if (need <= excl + h0) {
-        s_bin = 2 * t;
-        s_before = excl;
-        s_in_bin = h0;
-      } else {
-        s_bin = 2 * t + 1;
-        s_before = excl + h0;
-        s_in_bin = h1;
+      uint32_t before = excl;
+#pragma unroll
+      for (int b = 0; b < BPT; b++) {
+        if (need <= before + hv[b]) {
+          s_bin = BPT * t + b;
+          s_before = before;
+          s_in_bin = hv[b];
+          break;
+        }
+        before += hv[b];
       }
     }
     __syncthreads();
@@ -683,13 +698,19 @@ void launch_select_rows(const SelectArgs& a, uint64_t rows, uint64_t* scratch,
     launched();
     return;
   }
+  // short uniform rows: 256 threads per row, several rows per SM
+  if (!a.row_off && a.n <= kShortRow && a.k <= kShortCap) {
+    select_rows_kernel<256, kShortCap><<<(unsigned)rows, 256, 0, stream>>>(a, nullptr, 0);
+    launched();
+    return;
+  }
   uint32_t stride = 0;
   if (a.k > kSelectSmemCap) {
     uint64_t len = 1;
     while (len < a.k) len <<= 1;
     stride = (uint32_t)len;
   }
-  select_rows_kernel<<<(unsigned)rows, kSelThreads, 0, stream>>>(a, scratch, stride);
+  select_rows_kernel<kSelThreads, kSelectSmemCap><<<(unsigned)rows, kSelThreads, 0, stream>>>(a, scratch, stride);
   launched();
 }
 
