@@ -693,7 +693,8 @@ uint32_t engine_two_stage(const Index& rq, const Index& s1, const float* d_q, ui
   w.mark(st, 4);
   uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
   uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
-  select_rows(w, keys, w.sel_ids.as<uint32_t>(), off, 0, 0, nq, ke, 32, bits_for(rq.n - 1), ok, oi, st);
+  // rows are uniform (me candidates each): the strided form, not offsets
+  select_rows(w, keys, w.sel_ids.as<uint32_t>(), nullptr, me, me, nq, ke, 32, bits_for(rq.n - 1), ok, oi, st);
   w.mark(st, 5);
   return ke;
 }
