@@ -172,3 +172,38 @@ def test_server_config_is_validated_before_device_use():
     assert L.ovb_server_new(C.byref(cfg), C.byref(h)) == 2
     assert L.ovb_server_submit(None, 0, None, 0, 1, 0, C.byref(C.c_uint64())) == 1
     L.ovb_server_free(None)  # NULL is a no-op
+
+
+def test_ovr_loader_validates_rows_before_device_use(tmp_path):
+    """src/rank_io.rs:581-633: OVR1 rows must be permutations of [0, dim); a
+    row with a value >= dim or a repeated value, and trailing bytes, are
+    CORRUPT_INDEX.  ABI v1's loader refuses the format outright."""
+    L = lib()
+    head = b"OVR1" + bytes([1, 4, 0, 0, 0, 1, 0, 0, 0])
+    good = head + bytes([0, 0, 1, 0, 2, 0, 3, 0])
+    for name, data in (("trailing", good + b"\0"), ("range", head + bytes([0, 0, 1, 0, 2, 0, 4, 0])),
+                       ("repeat", head + bytes([0, 0, 1, 0, 1, 0, 3, 0])), ("short", good[:-1])):
+        p = _write(tmp_path / f"{name}.ovr", data)
+        out = C.c_void_p()
+        assert L.ovb_index_load_any(p.encode(), 0, C.byref(out)) == 5, name
+        assert not out.value
+    p = _write(tmp_path / "good.ovr", good)
+    out = C.c_void_p()
+    assert L.ordvec_index_load(p.encode(), 0, C.byref(out)) == 4
+
+
+def test_rank_and_selftest_entry_points_fail_cleanly_without_a_gpu():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    L = lib()
+    out = C.c_void_p()
+    assert L.ovb_rank_new(1, C.byref(out)) in (2, 11)  # bad dim, or no device first
+    assert L.ovb_rank_new(64, None) == 1
+    t, w = C.c_uint32(), C.c_uint64()
+    assert L.ovb_selftest_bounded_wait(None, None) == 1
+    assert L.ovb_selftest_bounded_wait(C.byref(t), C.byref(w)) == 11
+    assert L.ovb_index_search_device(None, 0, None, 0, 1, None, None, None) == 1
