@@ -51,21 +51,29 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int q = 0; q < QT; q++) acc[q] = 0;
     const uint4* src = (const uint4*)(blocks + blk * (uint64_t)lut_bytes) + lane;
-    for (uint32_t g = 0; g < G; g++) {
-      const uint4 c = __ldcs(src + g * 32);
-      const uint32_t cw[4] = {c.x, c.y, c.z, c.w};
-      const uint8_t* L = slut + g * 32 * 16;
+    // four 16-byte code loads in flight per lane: a warp usually scores one
+    // block, so one load at a time would leave it waiting on memory latency
+    for (uint32_t g0 = 0; g0 < G; g0 += 4) {
+      uint4 cv[4];
 #pragma unroll
-      for (int q = 0; q < QT; q++) {
-        const uint8_t* Lq = L + q * lut_bytes;
-        uint32_t a = 0;
+      for (int u = 0; u < 4; u++) cv[u] = g0 + u < G ? __ldcs(src + (g0 + u) * 32) : make_uint4(0, 0, 0, 0);
 #pragma unroll
-        for (int b = 0; b < 16; b++) {
-          const uint32_t byte = (cw[b >> 2] >> (8 * (b & 3))) & 0xFF;
-          a += Lq[(2 * b) * 16 + (byte & 15)];
-          a += Lq[(2 * b + 1) * 16 + (byte >> 4)];
+      for (int u = 0; u < 4; u++) {
+        if (g0 + u >= G) break;
+        const uint32_t cw[4] = {cv[u].x, cv[u].y, cv[u].z, cv[u].w};
+        const uint8_t* L = slut + (g0 + u) * 32 * 16;
+#pragma unroll
+        for (int q = 0; q < QT; q++) {
+          const uint8_t* Lq = L + q * lut_bytes;
+          uint32_t a = 0;
+#pragma unroll
+          for (int b = 0; b < 16; b++) {
+            const uint32_t byte = (cw[b >> 2] >> (8 * (b & 3))) & 0xFF;
+            a += Lq[(2 * b) * 16 + (byte & 15)];
+            a += Lq[(2 * b + 1) * 16 + (byte >> 4)];
+          }
+          acc[q] += a;
         }
-        acc[q] += a;
       }
     }
     const uint64_t doc = blk * 32 + lane;
