@@ -1,22 +1,32 @@
-"""Benchmark: FastScan top-1000 -> RankQuant b=2 rerank (k=10) over N=171,332
-dim-1024 docs -- the FastScan two-stage configuration -- on B200.
+"""Benchmark: the large-corpus configuration on B200 -- Bitmap (n_top=192)
+top-2,000 candidates -> RankQuant b=2 asymmetric rerank, top-100, over
+N=10,000,000 dim-768 docs resident in HBM, batches of 1,024 queries.
 
-One step = one batch of 1000 synthetic queries through the whole two-stage
+One step = one batch of 1,024 synthetic queries through the whole two-stage
 path.  Prints ONE JSON line (rank 0).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-value  : device-timed QPS of the batched form (all queries of a step in one
+value  : device-timed QPS of the batched form (each step's 1,024 queries in one
          fused call), queries resident in HBM; L2 flushed (256 MiB write)
-         between steps, outside the timed region.
+         between steps, outside the timed region (the 0.96 GB of bitmap codes
+         and the 1.92 GB of RankQuant codes exceed L2 anyway).
 e2e    : the same step through the public C ABI (ovb_two_stage_search) from
-         pinned host buffers: H2D of the queries and D2H of the top-10 inside
+         pinned host buffers: H2D of the queries and D2H of the top-100 inside
          the timed region.
-plain  : one query per launch (device pointers), p50/p99 latency and QPS, and
-         whether its top-10 ids equal the batched form's.
-cpu_baseline / --impl reference: the CPU oracle's AVX-512 + OpenMP restatement
-         of the reference path (the Rust crate cannot be built here), all host
-         threads, on a bounded query sample.
+plain  : one query per call (device pointers), p50/p99 and QPS, and whether its
+         top-100 ids equal the batched form's.
+roofline: the dominant kernel, bitmap_pair_kernel (the stage-1 overlap scan as
+         a u8 GEMM on tcgen05), timed by the stage events of every timed step.
+cpu_baseline / --impl reference: the oracle's AVX-512 + OpenMP restatement of
+         the reference path (Bitmap::top_m_candidates_batched_chunked in groups
+         of 8 queries, then the AVX-512 subset rerank), all host threads, on a
+         bounded query sample; the reference arm builds its inputs with the
+         oracle's restatement of the corpus generator and never loads the
+         product library.
+Extra keys (one GPU): the multi-bucket stage-1 variant of the same corpus, the
+FastScan two-stage configuration (N=171,332, dim 1024), the mixed-k/bits batch,
+the sign->b1 configuration, the three-index serving loop and the Rank modes.
 """
 from __future__ import annotations
 
@@ -36,14 +46,37 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "QPS & scan HBM GB/s vs peak, batched vs plain GPU @ identical top-10; p50/p99 ms"
-N_DOCS, DIM, NQ, K, M = 171_332, 1024, 1000, 10, 1000
-SEED = 0x0DD5EED2
+# headline workload: the large-corpus configuration
+N_DOCS, DIM, NQ, K, M, N_TOP, BITS = 10_000_000, 768, 1024, 100, 2000, 192, 2
+QPV = DIM // 64
+SEED = 0x0DD5EED4  # corpus; queries use SEED + 1 (+1000 per rank)
+BUILD_CHUNK = 1_000_000
 STAGES = ["prep", "threshold", "scan", "select", "rerank", "final_select"]
-# DRAM traffic of one filter launch of fastscan_persist_kernel at this workload, from an ncu capture
-# (52,310,016 B read + 2,875,392 B written): the codes and LUTs cross HBM about once.
-TC_FILTER_DRAM_BYTES = 52_310_016 + 2_875_392
-WORKLOAD = (f"fastscan_two_stage: RankQuantFastscan top-{M} -> RankQuant b=2 asymmetric rerank top-{K}; "
-            f"N={N_DOCS} dim={DIM}; {NQ} queries per step")
+WORKLOAD = (f"large_corpus_bitmap_two_stage: Bitmap n_top={N_TOP} top-{M} -> RankQuant b={BITS} asymmetric "
+            f"rerank top-{K}; N={N_DOCS} dim={DIM}; {NQ} queries per step")
+# DRAM traffic of one filter launch of bitmap_pair_kernel at this workload (ncu
+# dram__bytes_read.sum + dram__bytes_write.sum): the codes cross HBM about once.
+PAIR_FILTER_DRAM_BYTES = None
+# FastScan two-stage configuration (extra key)
+FS_N, FS_DIM, FS_NQ, FS_K, FS_M, FS_SEED = 171_332, 1024, 1000, 10, 1000, 0x0DD5EED2
+# DRAM traffic of one filter launch of fastscan_persist_kernel at that workload, from an ncu capture
+# (52,310,016 B read + 2,875,392 B written).
+FS_TC_FILTER_DRAM_BYTES = 52_310_016 + 2_875_392
+# the reference arm keeps its whole run (warm-up + timed steps) near this many seconds
+REFERENCE_BUDGET_S = 150.0
+
+
+def headline_config(world: int) -> dict:
+    return {"workload": WORKLOAD, "n_docs": N_DOCS, "dim": DIM, "queries_per_step_per_gpu": NQ, "k": K,
+            "candidates": M, "stage1": f"Bitmap n_top={N_TOP} (constant weight)", "rerank": f"RankQuant b={BITS}",
+            "form": "batched (one fused two-stage call per step)",
+            "l2": "inputs larger than L2 (0.96 GB bitmap + 1.92 GB RankQuant codes) and a 256 MiB device write "
+                  "between steps, outside the timed region",
+            "parallelism": f"replicas x{world} (queries sharded per rank, no data-path collective)"}
+
+
+def query_seed(rank: int) -> int:
+    return SEED + 1 + 1000 * rank
 
 
 def measured_peaks():
@@ -98,7 +131,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-# ------------------------------------------------------------ CPU baseline
+# ------------------------------------------------------------ CPU helpers
 def cpu_model() -> str:
     try:
         with open("/proc/cpuinfo") as f:
@@ -110,62 +143,96 @@ def cpu_model() -> str:
     return "unknown"
 
 
-def cpu_two_stage_qps(docs, queries, budget_s: float):
-    """Time the oracle's AVX-512/OpenMP restatement on a bounded query sample."""
-    from oracle import oracle as orc
+def oracle_codes(orc, docs, first, words, packed):
+    """Oracle-encode a chunk of docs into the host code arrays (rows first..)."""
+    n = docs.shape[0]
+    orc.encode_bitmap_rankquant(docs, DIM, N_TOP, BITS, words[first * QPV:(first + n) * QPV],
+                                packed[first * DIM * BITS // 8:(first + n) * DIM * BITS // 8])
 
-    blocks = orc.fastscan_pack(docs, DIM)
-    packed = orc.rankquant_encode(docs, DIM, 2)
-    threads = orc.max_threads()
-    probe = min(len(queries), max(threads, 8))
-    t0 = time.perf_counter()
-    orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[:probe], M, K, threads)
-    dt = time.perf_counter() - t0
-    sample = int(min(len(queries), max(probe, probe * budget_s / max(dt, 1e-6))))
-    t0 = time.perf_counter()
-    s, i = orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[:sample], M, K, threads)
-    dt = time.perf_counter() - t0
-    # one thread, a small sample (about a second)
-    one = min(len(queries), 16)
-    t1 = time.perf_counter()
-    orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[:one], M, K, 1)
-    qps1 = one / (time.perf_counter() - t1)
-    return sample / dt, threads, sample, (s, i), blocks, packed, qps1
+
+def topk_agreement(orc, packed, dim, bits, queries, ids_a, ids_b):
+    """Compare two top-k id matrices of the same queries.  Returns (identical,
+    equal_up_to_fp64_near_ties, rows_differing): rows are ordered by FP64 score
+    (desc, id asc) and may differ only at positions whose FP64 scores are within
+    1e-5 * max(|s|, 1e-3) of each other (the float contract of the rerank)."""
+    same = bool(np.array_equal(ids_a, ids_b))
+    if same:
+        return True, True, 0
+    ok, rows = True, 0
+    for qi in range(ids_a.shape[0]):
+        a, b = ids_a[qi], ids_b[qi]
+        if np.array_equal(a, b):
+            continue
+        rows += 1
+        va, vb = a[a >= 0].astype(np.uint32), b[b >= 0].astype(np.uint32)
+        if va.size != vb.size:
+            ok = False
+            continue
+        sa = orc.rq_scores_f64_subset(packed, dim, bits, queries[qi], va)
+        sb = orc.rq_scores_f64_subset(packed, dim, bits, queries[qi], vb)
+        oa, ob_ = np.lexsort((va, -sa)), np.lexsort((vb, -sb))
+        sa, sb = sa[oa], sb[ob_]
+        tol = 1e-5 * np.maximum(np.maximum(np.abs(sa), np.abs(sb)), 1e-3)
+        if np.any(np.abs(sa - sb) > tol):
+            ok = False
+    return False, ok, rows
+
+
+def cpu_sample_size(probe_qps: float, budget_s: float, group: int, cap: int) -> int:
+    q = int(probe_qps * budget_s) // group * group
+    return max(group, min(cap, q))
+
+
+# ------------------------------------------------------------ reference arm
+def cpu_headline_inputs(orc):
+    """The headline corpus encoded on the host by the oracle (no product code):
+    bitmap words, RankQuant b=2 codes and rank 0's queries."""
+    words = np.empty(N_DOCS * QPV, np.uint64)
+    packed = np.empty(N_DOCS * DIM * BITS // 8, np.uint8)
+    for first in range(0, N_DOCS, BUILD_CHUNK):
+        n = min(BUILD_CHUNK, N_DOCS - first)
+        oracle_codes(orc, orc.synth_docs(SEED, n, DIM, first=first), first, words, packed)
+    queries, _ = orc.synth_queries(query_seed(0), N_DOCS, NQ, DIM)
+    return words, packed, queries
 
 
 def reference_arm(args):
     # the reference path is a CPU path: under torchrun rank 0 alone runs it
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    import ordvec_b200 as ob
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     from oracle import oracle as orc
 
-    docs = ob.synth_docs(SEED, N_DOCS, DIM)
-    queries, _ = ob.synth_queries(SEED, N_DOCS, NQ, DIM)
-    blocks = orc.fastscan_pack(docs, DIM)
-    packed = orc.rankquant_encode(docs, DIM, 2)
     threads = orc.max_threads()
-    # size each step so the whole run stays within a few minutes
     t0 = time.perf_counter()
-    orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[:threads], M, K, threads)
-    per_q = (time.perf_counter() - t0) / threads
-    per_step = int(max(threads, min(NQ, 20.0 / max(per_q, 1e-9) / max(args.steps + args.warmup, 1))))
+    words, packed, queries = cpu_headline_inputs(orc)
+    build_s = time.perf_counter() - t0
+    run = lambda qs: orc.cpu_bitmap_two_stage(words, packed, N_DOCS, DIM, N_TOP, BITS, qs, M, K, threads)
+    # size each step so the whole run stays within a few minutes
+    probe = min(NQ, 8 * threads)
+    t0 = time.perf_counter()
+    run(queries[:probe])
+    probe_qps = probe / (time.perf_counter() - t0)
+    per_step = cpu_sample_size(probe_qps, REFERENCE_BUDGET_S / max(args.steps + args.warmup, 1), 8, NQ)
+    span = NQ - per_step + 1
     for w in range(args.warmup):
-        orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[:per_step], M, K, threads)
+        run(queries[:per_step])
     t0 = time.perf_counter()
     done = 0
     for s in range(args.steps):
-        off = (s * per_step) % max(NQ - per_step + 1, 1)
-        orc.cpu_fastscan_two_stage(blocks, packed, N_DOCS, DIM, queries[off:off + per_step], M, K, threads)
+        off = (s * per_step) % span
+        run(queries[off:off + per_step])
         done += per_step
     dt = time.perf_counter() - t0
     qps = done / dt
-    line = {"impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": args.gpus,
+    line = {"impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(args.steps, 1),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8-lut/u32-acc/f32",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "queries_per_step_sampled": per_step},
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64-popc/f32",
+            "data": "synthetic", "config": headline_config(world),
             "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
-                             "sample": f"{per_step} queries per step x {args.steps} steps"},
+                             "sample": f"{per_step} of each step's {NQ} queries (rotating offsets) x {args.steps} "
+                                       f"steps, all host threads", "cpu_model": cpu_model(),
+                             "inputs_built_s": build_s},
             "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -272,107 +339,145 @@ def sign_plain_run(ob, torch, dev, plain_queries: int, cpu: bool):
         sample = min(nq, 200)
         orc.cpu_sign_two_stage(words, packed, n, dim, 1, queries[:8], m, k, threads)
         t0 = time.perf_counter()
-        orc.cpu_sign_two_stage(words, packed, n, dim, 1, queries[:sample], m, k, threads)
+        s, i = orc.cpu_sign_two_stage(words, packed, n, dim, 1, queries[:sample], m, k, threads)
         dt = time.perf_counter() - t0
+        same, tol_same, rows = topk_agreement(orc, packed, dim, 1, queries[:sample], ids[:sample], i)
         out["cpu_oracle"] = {"qps": sample / dt, "cores": threads, "sample": f"{sample} queries, one batch",
-                             "kind": "port (AVX-512 popcount + b1 LUT rerank)"}
+                             "kind": "port (AVX-512 popcount + b1 LUT rerank)",
+                             "identical_top10_vs_cpu": same, "equal_up_to_fp64_near_ties": tol_same,
+                             "rows_differing": rows}
     return out
 
 
-# ------------------------------------------------------------- large corpus
-def large_run(ob, torch, dev, steps: int, plain_queries: int):
-    """The large-corpus configuration: N=10,000,000 synthetic docs, dim 768,
-    RankQuant b=2 (1.92 GB of codes), constant-weight Bitmap n_top=192
-    (0.96 GB) and MultiBucketBitmap b=2 (3.84 GB) resident in HBM; batches of
-    1,024 queries, stage-1 top-2,000, rerank to top-100.  Per stage-1 kind:
-    device-timed batched QPS (queries resident in HBM), the plain form (one
-    query per call) with p50/p99, whether both give identical top-100 ids,
-    the stage breakdown, and the stage-1 scans against their rooflines (the
-    batched tensor-core overlap scan against the int8 tensor peak, the plain
-    popcount scan as HBM GB/s)."""
-    n, dim, seed, nq, m, k = 10_000_000, 768, 0x0DD5EED4, 1024, 2000, 100
-    t0 = time.perf_counter()
-    rq, bm, mb = ob.RankQuant(dim, 2), ob.Bitmap(dim, 192), ob.MultiBucketBitmap(dim, 2)
-    chunk = 1_000_000
-    for first in range(0, n, chunk):
-        d = ob.synth_docs(seed, min(chunk, n - first), dim, first=first)
-        for ix in (rq, bm, mb):
-            ix.add(d)
-    del d
-    build_s = time.perf_counter() - t0
-    queries, _ = ob.synth_queries(seed + 1, n, nq, dim)
+# ------------------------------------------------------------- FastScan cfg
+def fastscan_run(ob, torch, dev, args, cpu: bool):
+    """The FastScan two-stage configuration: N=171,332 synthetic docs (seed
+    0x0DD5EED2), dim 1024, RankQuantFastscan top-1,000 -> RankQuant b=2
+    asymmetric rerank top-10, 1,000 queries per step.  Batched form
+    (device-timed, L2 flushed between steps), e2e through the C ABI from pinned
+    host buffers, the plain one-query form, the stage profile and rooflines,
+    the serving loop on this route, and the CPU oracle (AVX-512 VPSHUFB
+    FastScan + AVX-512 rerank, all host threads) on a bounded sample with the
+    identity of its top-10 against the batched GPU result."""
+    from ordvec_b200._lib import check, lib
+
+    docs = ob.synth_docs(FS_SEED, FS_N, FS_DIM)
+    queries, _ = ob.synth_queries(FS_SEED, FS_N, FS_NQ, FS_DIM)
+    rq = ob.RankQuant(FS_DIM, 2)
+    rq.add(docs)
+    fs = ob.RankQuantFastscan(FS_DIM)
+    fs.add(docs)
     d_q = torch.from_numpy(queries).to(dev)
-    d_s = torch.empty(nq * k, dtype=torch.float32, device=dev)
-    d_i = torch.empty(nq * k, dtype=torch.int64, device=dev)
+    d_s = torch.empty(FS_NQ * FS_K, dtype=torch.float32, device=dev)
+    d_i = torch.empty(FS_NQ * FS_K, dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
-    hbm_peak, bf16_peak, peak_kind = measured_peaks()
-    out = {"workload": f"N={n} dim={dim}: RankQuant b=2 + Bitmap n_top=192 + MultiBucketBitmap b=2 resident; "
-                       f"{nq} queries per batch, stage-1 top-{m} -> rerank top-{k}",
-           "build_s": build_s, "code_bytes": {"rankquant_b2": n * 192, "bitmap": n * 96, "multibucket": n * 384}}
-    clocks = ClockSampler(dev.index or 0)
-    clocks.start()
-    time.sleep(0.3)
-    for name, s1, words in (("bitmap", bm, 12), ("multibucket", mb, 48)):
-        def run(cnt, qp, sp_, ip):
-            ob.two_stage_search_device(rq, s1, qp, cnt, m, k, sp_, ip, sp)
 
-        for _ in range(3):
-            run(nq, d_q.data_ptr(), d_s.data_ptr(), d_i.data_ptr())
-        reps = max(3, min(steps, 10))
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
-        for r in range(reps):  # the codes (> L2) stream from HBM in every batch
-            ev[r][0].record(stream)
-            run(nq, d_q.data_ptr(), d_s.data_ptr(), d_i.data_ptr())
-            ev[r][1].record(stream)
+    def step(nq=FS_NQ, q_ptr=None, s_ptr=None, i_ptr=None):
+        ob.two_stage_search_device(rq, fs, q_ptr or d_q.data_ptr(), nq, FS_M, FS_K, s_ptr or d_s.data_ptr(),
+                                   i_ptr or d_i.data_ptr(), sp)
+
+    for _ in range(3):
+        step()
+    steps = max(args.steps, 5)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for s in range(steps):
+        flush.fill_(s & 0xFF)
+        ev[s][0].record(stream)
+        step()
+        ev[s][1].record(stream)
+    torch.cuda.synchronize(dev)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    batched_ids = d_i.view(FS_NQ, FS_K).cpu().numpy()
+    # e2e: C ABI, pinned host buffers
+    h_q = torch.from_numpy(queries).pin_memory()
+    h_s = torch.empty(FS_NQ * FS_K, dtype=torch.float32).pin_memory()
+    h_i = torch.empty(FS_NQ * FS_K, dtype=torch.int64).pin_memory()
+    e2e_ms = []
+    for s in range(3 + 50):
+        flush.fill_(s & 0xFF)
         torch.cuda.synchronize(dev)
-        batch_ms = statistics.median(a.elapsed_time(b) for a, b in ev)
-        ids = d_i.view(nq, k).cpu().numpy()
-        P = max(4, min(plain_queries, 32))
-        p_s = torch.empty(P * k, dtype=torch.float32, device=dev)
-        p_i = torch.empty(P * k, dtype=torch.int64, device=dev)
-        run(1, d_q[0].data_ptr(), p_s.data_ptr(), p_i.data_ptr())
-        pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(P)]
-        for qi in range(P):
-            pev[qi][0].record(stream)
-            run(1, d_q[qi].data_ptr(), p_s[qi * k:].data_ptr(), p_i[qi * k:].data_ptr())
-            pev[qi][1].record(stream)
-        torch.cuda.synchronize(dev)
-        plain_ms = [a.elapsed_time(b) for a, b in pev]
-        same = bool(np.array_equal(p_i.view(P, k).cpu().numpy(), ids[:P]))
-        st = ob.two_stage_profile(rq, s1, d_q.data_ptr(), nq, m, k, d_s.data_ptr(), d_i.data_ptr(), sp)
-        st1 = ob.two_stage_profile(rq, s1, d_q.data_ptr(), 1, m, k, p_s.data_ptr(), p_i.data_ptr(), sp)
-        ops = 2 * n * nq * words * 64  # 0/1-byte AND-overlap MACs, multiply + add
-        tops = ops / (st[2] * 1e-3) / 1e12
-        plain_gbs = n * words * 8 / (st1[2] * 1e-3) / 1e9
-        out[name] = {
-            "batched_qps": nq / (batch_ms * 1e-3), "batch_ms": batch_ms,
-            "plain_qps": 1e3 / statistics.mean(plain_ms), "plain_p50_ms": float(np.percentile(plain_ms, 50)),
-            "plain_p99_ms": float(np.percentile(plain_ms, 99)), "plain_queries": P,
-            "batched_over_plain": nq / (batch_ms * 1e-3) * statistics.mean(plain_ms) * 1e-3,
-            "identical_top100_batched_vs_plain": same,
-            "stages_ms": dict(zip(STAGES, st)), "stages_ms_plain": dict(zip(STAGES, st1)),
-            "roofline_batched_scan": {"bound": "tensor", "kernel": "bitmap_tc_kernel (filter epilogue)",
-                                      "achieved": tops, "peak": 2 * bf16_peak, "unit": "TOPS (int8)",
-                                      "frac": tops / (2 * bf16_peak),
-                                      "codes_gbs": n * words * 8 * ((nq + 255) // 256) / (st[2] * 1e-3) / 1e9,
-                                      "peak_source": f"2 x {peak_kind} bf16 dense TFLOP/s (burst)"},
-            "roofline_plain_scan": {"bound": "hbm", "kernel": "popc_scan_kernel / multibucket_scan_kernel",
-                                    "achieved": plain_gbs, "peak": hbm_peak, "unit": "GB/s",
-                                    "frac": plain_gbs / hbm_peak, "peak_source": f"{peak_kind} HBM copy"},
-        }
-    out["clocks"] = clocks.stop()
+        t0 = time.perf_counter()
+        check(lib().ovb_two_stage_search(rq.handle, fs.handle, C.c_void_p(h_q.data_ptr()), FS_NQ, FS_M, FS_K,
+                                         C.c_void_p(h_s.data_ptr()), C.c_void_p(h_i.data_ptr())))
+        if s >= 3:
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    # plain
+    P = min(args.plain_queries, FS_NQ)
+    pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(P)]
+    p_s = torch.empty(P * FS_K, dtype=torch.float32, device=dev)
+    p_i = torch.empty(P * FS_K, dtype=torch.int64, device=dev)
+    for qi in range(3):
+        step(1, d_q[qi].data_ptr(), p_s[qi * FS_K:].data_ptr(), p_i[qi * FS_K:].data_ptr())
+    for qi in range(P):
+        flush.fill_(qi & 0xFF)
+        pev[qi][0].record(stream)
+        step(1, d_q[qi].data_ptr(), p_s[qi * FS_K:].data_ptr(), p_i[qi * FS_K:].data_ptr())
+        pev[qi][1].record(stream)
+    torch.cuda.synchronize(dev)
+    plain_ms = [a.elapsed_time(b) for a, b in pev]
+    identical = bool(np.array_equal(p_i.view(P, FS_K).cpu().numpy(), batched_ids[:P]))
+    st = ob.two_stage_profile(rq, fs, d_q.data_ptr(), FS_NQ, FS_M, FS_K, d_s.data_ptr(), d_i.data_ptr(), sp)
+    st1 = ob.two_stage_profile(rq, fs, d_q.data_ptr(), 1, FS_M, FS_K, d_s.data_ptr(), d_i.data_ptr(), sp)
+    hbm_peak, bf16_peak, peak_kind = measured_peaks()
+    pairs_pad = ((FS_DIM // 2 + 31) // 32) * 32
+    code_bytes = ((FS_N + 31) // 32) * 16 * pairs_pad
+    ops = 2 * FS_N * FS_NQ * pairs_pad * 16
+    plain_bytes = code_bytes + pairs_pad * 16 + FS_N * 4
+    batched_qps = FS_NQ / (statistics.mean(step_ms) * 1e-3)
+    out = {"workload": f"fastscan_two_stage: RankQuantFastscan top-{FS_M} -> RankQuant b=2 rerank top-{FS_K}; "
+                       f"N={FS_N} dim={FS_DIM}; {FS_NQ} queries per call",
+           "batched_qps": batched_qps, "batched_ms": statistics.mean(step_ms),
+           "e2e_qps": FS_NQ / (statistics.mean(e2e_ms) * 1e-3), "e2e_calls": len(e2e_ms),
+           "e2e_top10_equal_to_device_path": bool(np.array_equal(h_i.numpy().reshape(FS_NQ, FS_K), batched_ids)),
+           "plain": {"qps": 1e3 / statistics.mean(plain_ms), "p50_ms": float(np.percentile(plain_ms, 50)),
+                     "p99_ms": float(np.percentile(plain_ms, 99)), "queries": P,
+                     "identical_top10_vs_batched": identical},
+           "stages_ms": dict(zip(STAGES, st)), "stages_ms_plain": dict(zip(STAGES, st1)),
+           "roofline_batched_scan": {"bound": "tensor", "kernel": "fastscan_persist_kernel (filter epilogue)",
+                                     "achieved": ops / (st[2] * 1e-3) / 1e12, "peak": 2 * bf16_peak,
+                                     "unit": "TOPS (int8)", "frac": ops / (st[2] * 1e-3) / 1e12 / (2 * bf16_peak),
+                                     "traffic": FS_TC_FILTER_DRAM_BYTES,
+                                     "peak_source": f"2 x {peak_kind} bf16 dense TFLOP/s (burst)"},
+           "roofline_plain_scan": {"bound": "hbm", "kernel": "fastscan_scan_kernel",
+                                   "achieved": plain_bytes / (st1[2] * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                                   "frac": plain_bytes / (st1[2] * 1e-3) / 1e9 / hbm_peak,
+                                   "peak_source": f"{peak_kind} HBM copy"}}
+    if args.serve_seconds > 0:
+        out["serving"] = serving_run(ob, rq, fs, queries, batched_ids, args.serve_seconds, args.serve_rate)
+    if cpu:
+        from oracle import oracle as orc
+
+        blocks = orc.fastscan_pack(docs, FS_DIM)
+        packed = orc.rankquant_encode(docs, FS_DIM, 2)
+        out["codes_identical_to_oracle"] = bool(np.array_equal(fs.payload(), blocks)
+                                                and np.array_equal(rq.payload(), packed))
+        threads = orc.max_threads()
+        probe = min(FS_NQ, max(threads, 8))
+        t0 = time.perf_counter()
+        orc.cpu_fastscan_two_stage(blocks, packed, FS_N, FS_DIM, queries[:probe], FS_M, FS_K, threads)
+        sample = cpu_sample_size(probe / (time.perf_counter() - t0), args.cpu_seconds / 2, 8, FS_NQ)
+        t0 = time.perf_counter()
+        s, i = orc.cpu_fastscan_two_stage(blocks, packed, FS_N, FS_DIM, queries[:sample], FS_M, FS_K, threads)
+        dt = time.perf_counter() - t0
+        same, tol_same, rows = topk_agreement(orc, packed, FS_DIM, 2, queries[:sample], batched_ids[:sample], i)
+        out["cpu_oracle"] = {"qps": sample / dt, "cores": threads, "kind": "port",
+                             "sample": f"first {sample} of the {FS_NQ} queries, all host threads",
+                             "identical_top10_vs_cpu": same, "equal_up_to_fp64_near_ties": tol_same,
+                             "rows_differing": rows}
     return out
 
 
 # ----------------------------------------------------- Rank and symmetric
-def rank_modes_run(ob, torch, dev, rq, queries, plain_queries: int):
+def rank_modes_run(ob, torch, dev, plain_queries: int):
     """The Rank (u16) index and RankQuant's symmetric search, device-timed
     through ob.search_device: Rank(768) over N=1,000,000 synthetic docs
-    (1.54 GB of ranks) and this benchmark's RankQuant b=2 index, one query per
-    call (plain) and a batch per call.  For the plain calls the whole call's
-    time is set against the bytes the scan must read (ranks or codes once, plus
-    the 4-byte key row), a lower bound on the scan kernel's HBM rate."""
+    (1.54 GB of ranks) and a RankQuant b=2 dim-1024 index over N=171,332, one
+    query per call (plain) and a batch per call.  For the plain calls the whole
+    call's time is set against the bytes the scan must read (ranks or codes
+    once, plus the 4-byte key row), a lower bound on the scan kernel's HBM
+    rate."""
     hbm_peak, _, peak_kind = measured_peaks()
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
@@ -412,33 +517,35 @@ def rank_modes_run(ob, torch, dev, rq, queries, plain_queries: int):
             "plain_p50_ms": float(np.percentile(plain, 50)), "batched_qps": nb / (statistics.median(batch) * 1e-3),
             "batch_queries": nb, "roofline_plain_call": roof(n * dim * 2 + 4 * n, statistics.median(plain))}
     del rk
+    rq = ob.RankQuant(FS_DIM, 2)
+    rq.add(ob.synth_docs(FS_SEED, FS_N, FS_DIM))
+    queries, _ = ob.synth_queries(FS_SEED, FS_N, 1000, FS_DIM)
     nr = len(rq)
     d_q = torch.from_numpy(queries).to(dev)
     plain = timed(rq, d_q, 1, 10, False, P)
-    nbq = min(1000, d_q.shape[0])
-    batch = timed(rq, d_q, nbq, 10, False, 3)
+    batch = timed(rq, d_q, 1000, 10, False, 3)
     out["rankquant_symmetric"] = {
-        "workload": f"RankQuant b={rq.bits} dim={rq.dim} N={nr} (this benchmark's corpus) symmetric top-10",
+        "workload": f"RankQuant b={rq.bits} dim={rq.dim} N={nr} symmetric top-10",
         "plain_qps": 1e3 / statistics.mean(plain), "plain_p50_ms": float(np.percentile(plain, 50)),
-        "batched_qps": nbq / (statistics.median(batch) * 1e-3), "batch_queries": nbq,
+        "batched_qps": 1000 / (statistics.median(batch) * 1e-3), "batch_queries": 1000,
         "roofline_plain_call": roof(nr * rq.dim * rq.bits // 8 + 4 * nr, statistics.median(plain))}
     return out
 
 
 # ------------------------------------------------------------------ serving
 def serving_run(ob, rq, fs, queries, batched_ids, seconds: float, rate_qps: float):
-    """The serving loop on this workload's route: seeded Poisson request
-    arrivals offering `rate_qps` queries/s, 1-256 queries per request, k=10,
-    m=1000; answered by ob.Server (continuous batching, 3 worker streams).
-    Reports completed QPS, request latency p50/p99 and whether every answer
-    equals the batched form's top-10."""
+    """The serving loop on the FastScan route: seeded Poisson request arrivals
+    offering `rate_qps` queries/s, 1-256 queries per request, k=10, m=1000;
+    answered by ob.Server (continuous batching, 3 worker streams).  Reports
+    completed QPS, request latency p50/p99 and whether every answer equals the
+    batched form's top-10."""
     import threading
 
-    rng = np.random.default_rng(SEED)
+    rng = np.random.default_rng(FS_SEED)
     mean_size = 128.5
     n_req = max(int(seconds * rate_qps / mean_size), 8)
     sizes = rng.integers(1, 257, n_req)
-    offs = rng.integers(0, NQ - 256, n_req)
+    offs = rng.integers(0, FS_NQ - 256, n_req)
     gaps = rng.exponential(mean_size / rate_qps, n_req)
     srv = ob.Server(workers=3, max_batch=1024)
     route = srv.add_route(rq, fs)
@@ -453,7 +560,7 @@ def serving_run(ob, rq, fs, queries, batched_ids, seconds: float, rate_qps: floa
             res, lat[j] = tickets[j].wait()
             done_at[j] = time.perf_counter()
             o, sz = int(offs[j]), int(sizes[j])
-            if not np.array_equal(res.indices.reshape(sz, K), batched_ids[o:o + sz]):
+            if not np.array_equal(res.indices.reshape(sz, FS_K), batched_ids[o:o + sz]):
                 same[0] = False
 
     th = threading.Thread(target=collect)
@@ -465,14 +572,14 @@ def serving_run(ob, rq, fs, queries, batched_ids, seconds: float, rate_qps: floa
         while time.perf_counter() < due:
             pass
         o, sz = int(offs[j]), int(sizes[j])
-        tickets[j] = srv.submit(route, queries[o:o + sz], K, M)
+        tickets[j] = srv.submit(route, queries[o:o + sz], FS_K, FS_M)
     th.join()
     wall = max(done_at) - t0
     st = srv.stats()
     srv.close()
     n_q = int(sizes.sum())
     return {"offered_qps": rate_qps, "completed_qps": n_q / wall, "requests": n_req, "queries": n_q,
-            "request_queries": "uniform 1-256", "k": K, "candidates": M,
+            "request_queries": "uniform 1-256", "k": FS_K, "candidates": FS_M,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(np.mean(lat)), "batches": st["batches"],
             "max_concurrent_batches": st["max_concurrent_batches"], "workers": 3,
@@ -484,24 +591,41 @@ def serving_run(ob, rq, fs, queries, batched_ids, seconds: float, rate_qps: floa
 def profile_case(case: str):
     """Small single-kernel workloads for ncu captures (no timing, no JSON):
       bitmap    Bitmap(768, 192) top-2000 of 1024 queries, N=2M (bitmap_pair_kernel)
-      popc      the same index, one query per call (popc_rows_kernel, wide select)
+      bitmap10m the same at N=10M (the headline's stage-1 index only, 0.96 GB)
+      popc      the 2M index, one query per call (popc_rows_kernel, wide select)
       rank      RankQuant(1024, 2) exact top-100 of 1024 queries, N=1M (rank_tc_kernel)
-      fastscan  this workload's FastScan top-1000 of 1000 queries (fastscan_tc_kernel)
-      plain     this workload's two-stage search, one query per call, 12 calls
+      fastscan  the FastScan configuration's top-1000 of 1000 queries (fastscan_tc_kernel)
+      plain     the FastScan two-stage search, one query per call, 12 calls
                 (fastscan_scan_kernel, select_rows_cluster_kernel, rerank)
       rankfull  Rank(768) N=1M top-100: symmetric then asymmetric, 1 query and 64
                 queries per call (rank_tile_kernel)
+      multibucket MultiBucketBitmap(768, 2) N=2M: diagonal-weight top-2000 of 1
+                query per call (multibucket_rows_kernel), 3 calls
+      encode    RankQuant(768, 2).add of 1M docs, twice (rank_encode_kernel)
     Each search runs more than once so captures can skip the first call."""
     import ordvec_b200 as ob
 
-    if case in ("bitmap", "popc"):
-        n = 2_000_000
+    if case in ("bitmap", "popc", "bitmap10m"):
+        n = 10_000_000 if case == "bitmap10m" else 2_000_000
         bm = ob.Bitmap(768, 192)
         for first in range(0, n, 1_000_000):
             bm.add(ob.synth_docs(0x0DD5EED4, 1_000_000, 768, first=first))
         q, _ = ob.synth_queries(0x0DD5EED5, n, 1024, 768)
-        for _ in range(2 if case == "bitmap" else 3):
-            bm.top_m_candidates_batched(q, 2000) if case == "bitmap" else bm.top_m_candidates(q[0], 2000)
+        for _ in range(3 if case == "popc" else 2):
+            bm.top_m_candidates(q[0], 2000) if case == "popc" else bm.top_m_candidates_batched(q, 2000)
+    elif case == "multibucket":
+        n = 2_000_000
+        mb = ob.MultiBucketBitmap(768, 2)
+        for first in range(0, n, 1_000_000):
+            mb.add(ob.synth_docs(0x0DD5EED4, 1_000_000, 768, first=first))
+        q, _ = ob.synth_queries(0x0DD5EED5, n, 4, 768)
+        for i in range(3):
+            mb.top_m_bilinear_batched(q[i:i + 1], mb.diagonal_weights(), 2000)
+    elif case == "encode":
+        rq = ob.RankQuant(768, 2)
+        d = ob.synth_docs(0x0DD5EED4, 1_000_000, 768)
+        for _ in range(2):
+            rq.add(d)
     elif case == "rank":
         n = 1_000_000
         rq = ob.RankQuant(1024, 2)
@@ -510,19 +634,19 @@ def profile_case(case: str):
         for _ in range(2):
             rq.search_asymmetric(q, 100)
     elif case == "fastscan":
-        fs = ob.RankQuantFastscan(DIM)
-        fs.add(ob.synth_docs(SEED, N_DOCS, DIM))
-        q, _ = ob.synth_queries(SEED + 1, N_DOCS, NQ, DIM)
+        fs = ob.RankQuantFastscan(FS_DIM)
+        fs.add(ob.synth_docs(FS_SEED, FS_N, FS_DIM))
+        q, _ = ob.synth_queries(FS_SEED + 1, FS_N, FS_NQ, FS_DIM)
         for _ in range(2):
-            fs.search(q, M)
+            fs.search(q, FS_M)
     elif case == "plain":
-        rq, fs = ob.RankQuant(DIM, 2), ob.RankQuantFastscan(DIM)
-        docs = ob.synth_docs(SEED, N_DOCS, DIM)
+        rq, fs = ob.RankQuant(FS_DIM, 2), ob.RankQuantFastscan(FS_DIM)
+        docs = ob.synth_docs(FS_SEED, FS_N, FS_DIM)
         rq.add(docs)
         fs.add(docs)
-        q, _ = ob.synth_queries(SEED + 1, N_DOCS, 12, DIM)
+        q, _ = ob.synth_queries(FS_SEED + 1, FS_N, 12, FS_DIM)
         for i in range(12):
-            ob.two_stage_search(rq, fs, q[i:i + 1], M, K)
+            ob.two_stage_search(rq, fs, q[i:i + 1], FS_M, FS_K)
     elif case == "rankfull":
         n = 1_000_000
         rk = ob.Rank(768)
@@ -636,24 +760,97 @@ def serving_multi_run(ob, seconds: float, rates):
     return out
 
 
+# ------------------------------------------------------------ headline build
+def build_headline(ob, orc, with_multibucket: bool):
+    """The headline indices built on the device in 1M-doc chunks; with an oracle
+    module, the same chunks are also encoded on the host by the oracle (bitmap
+    words and RankQuant b=2 codes, for the CPU leg and the code identity check)."""
+    rq, bm = ob.RankQuant(DIM, BITS), ob.Bitmap(DIM, N_TOP)
+    mb = ob.MultiBucketBitmap(DIM, BITS) if with_multibucket else None
+    words = np.empty(N_DOCS * QPV, np.uint64) if orc else None
+    packed = np.empty(N_DOCS * DIM * BITS // 8, np.uint8) if orc else None
+    for first in range(0, N_DOCS, BUILD_CHUNK):
+        d = ob.synth_docs(SEED, min(BUILD_CHUNK, N_DOCS - first), DIM, first=first)
+        for ix in (rq, bm, mb):
+            if ix is not None:
+                ix.add(d)
+        if orc:
+            oracle_codes(orc, d, first, words, packed)
+    return rq, bm, mb, words, packed
+
+
+def second_stage1_run(ob, torch, dev, rq, s1, name, words_per_doc, d_q, queries, plain_queries):
+    """Batched vs plain for one more stage-1 kind on the headline corpus."""
+    hbm_peak, bf16_peak, peak_kind = measured_peaks()
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    nq = d_q.shape[0]
+    d_s = torch.empty(nq * K, dtype=torch.float32, device=dev)
+    d_i = torch.empty(nq * K, dtype=torch.int64, device=dev)
+    run = lambda cnt, qp, s_, i_: ob.two_stage_search_device(rq, s1, qp, cnt, M, K, s_, i_, sp)
+    for _ in range(2):
+        run(nq, d_q.data_ptr(), d_s.data_ptr(), d_i.data_ptr())
+    reps = 3
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for r in range(reps):
+        ev[r][0].record(stream)
+        run(nq, d_q.data_ptr(), d_s.data_ptr(), d_i.data_ptr())
+        ev[r][1].record(stream)
+    torch.cuda.synchronize(dev)
+    batch_ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+    ids = d_i.view(nq, K).cpu().numpy()
+    P = max(4, min(plain_queries, 16))
+    p_s = torch.empty(P * K, dtype=torch.float32, device=dev)
+    p_i = torch.empty(P * K, dtype=torch.int64, device=dev)
+    run(1, d_q[0].data_ptr(), p_s.data_ptr(), p_i.data_ptr())
+    pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(P)]
+    for qi in range(P):
+        pev[qi][0].record(stream)
+        run(1, d_q[qi].data_ptr(), p_s[qi * K:].data_ptr(), p_i[qi * K:].data_ptr())
+        pev[qi][1].record(stream)
+    torch.cuda.synchronize(dev)
+    plain_ms = [a.elapsed_time(b) for a, b in pev]
+    st = ob.two_stage_profile(rq, s1, d_q.data_ptr(), nq, M, K, d_s.data_ptr(), d_i.data_ptr(), sp)
+    st1 = ob.two_stage_profile(rq, s1, d_q.data_ptr(), 1, M, K, p_s.data_ptr(), p_i.data_ptr(), sp)
+    ops = 2 * N_DOCS * nq * words_per_doc * 64
+    plain_gbs = N_DOCS * words_per_doc * 8 / (st1[2] * 1e-3) / 1e9
+    return {"workload": f"{name} top-{M} -> RankQuant b={BITS} rerank top-{K}; N={N_DOCS} dim={DIM}; "
+                        f"{nq} queries per batch",
+            "batched_qps": nq / (batch_ms * 1e-3), "batch_ms": batch_ms,
+            "plain_qps": 1e3 / statistics.mean(plain_ms), "plain_p50_ms": float(np.percentile(plain_ms, 50)),
+            "plain_p99_ms": float(np.percentile(plain_ms, 99)), "plain_queries": P,
+            "batched_over_plain": nq / (batch_ms * 1e-3) * statistics.mean(plain_ms) * 1e-3,
+            "identical_top100_batched_vs_plain": bool(np.array_equal(p_i.view(P, K).cpu().numpy(), ids[:P])),
+            "stages_ms": dict(zip(STAGES, st)), "stages_ms_plain": dict(zip(STAGES, st1)),
+            "roofline_batched_scan": {"bound": "tensor", "kernel": "bitmap_pair_kernel (filter epilogue)",
+                                      "achieved": ops / (st[2] * 1e-3) / 1e12, "peak": 2 * bf16_peak,
+                                      "unit": "TOPS (int8)", "frac": ops / (st[2] * 1e-3) / 1e12 / (2 * bf16_peak),
+                                      "peak_source": f"2 x {peak_kind} bf16 dense TFLOP/s (burst)"},
+            "roofline_plain_scan": {"bound": "hbm", "kernel": "multibucket_rows_kernel",
+                                    "achieved": plain_gbs, "peak": hbm_peak, "unit": "GB/s",
+                                    "frac": plain_gbs / hbm_peak, "peak_source": f"{peak_kind} HBM copy"}}
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--plain-queries", type=int, default=200)
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--plain-queries", type=int, default=100)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-rate", type=float, default=200_000.0, help="offered queries/s")
     ap.add_argument("--mixed-queries", type=int, default=-1,
                     help="also run the mixed-k/bits batch (N=1M, dim 1024) with this many queries; "
                          "0 = skip, -1 = 4096 on a single GPU")
-    ap.add_argument("--large", default="auto", choices=["auto", "on", "off"],
-                    help="also run the N=10M dim-768 bitmap / multi-bucket configuration (auto: one GPU only)")
-    ap.add_argument("--profile-case", choices=["bitmap", "popc", "rank", "fastscan", "plain", "rankfull"],
+    ap.add_argument("--extras", default="auto", choices=["auto", "on", "off"],
+                    help="the extra configurations (auto: on a single GPU only)")
+    ap.add_argument("--profile-case",
+                    choices=["bitmap", "bitmap10m", "popc", "rank", "fastscan", "plain", "rankfull", "multibucket",
+                             "encode"],
                     help="run one small kernel workload for an ncu capture and exit")
     args = ap.parse_args()
     if args.profile_case:
@@ -666,21 +863,24 @@ def main():
     import ordvec_b200 as ob
     from ordvec_b200._lib import check, lib
 
-    from ordvec_b200.replicas import ReplicaGroup, rank_env, shard_seed, whole_job_rate
+    from ordvec_b200.replicas import ReplicaGroup, rank_env, whole_job_rate
 
     rank, world, local = rank_env()
-    mixed_q = args.mixed_queries if args.mixed_queries >= 0 else (4096 if world == 1 else 0)
+    extras = (world == 1) if args.extras == "auto" else args.extras == "on"
+    mixed_q = args.mixed_queries if args.mixed_queries >= 0 else (4096 if extras else 0)
+    cpu = rank == 0 and not args.no_cpu
     torch.cuda.set_device(local)
     ob.set_device(local)
     dev = torch.device("cuda", local)
     group = ReplicaGroup("nccl", device=dev, sync=lambda: torch.cuda.synchronize(dev))
+    orc = None
+    if cpu:
+        from oracle import oracle as orc
 
-    docs = ob.synth_docs(SEED, N_DOCS, DIM)
-    queries, planted = ob.synth_queries(shard_seed(SEED, rank), N_DOCS, NQ, DIM)
-    rq = ob.RankQuant(DIM, 2)
-    rq.add(docs)
-    fs = ob.RankQuantFastscan(DIM)
-    fs.add(docs)
+    t0 = time.perf_counter()
+    rq, bm, mb, h_words, h_packed = build_headline(ob, orc, extras)
+    build_s = time.perf_counter() - t0
+    queries, _ = ob.synth_queries(query_seed(rank), N_DOCS, NQ, DIM)
 
     d_q = torch.from_numpy(queries).to(dev)
     d_s = torch.empty(NQ * K, dtype=torch.float32, device=dev)
@@ -690,7 +890,7 @@ def main():
     sp = stream.cuda_stream
 
     def step_device(nq=NQ, q_ptr=None, s_ptr=None, i_ptr=None):
-        ob.two_stage_search_device(rq, fs, q_ptr or d_q.data_ptr(), nq, M, K, s_ptr or d_s.data_ptr(),
+        ob.two_stage_search_device(rq, bm, q_ptr or d_q.data_ptr(), nq, M, K, s_ptr or d_s.data_ptr(),
                                    i_ptr or d_i.data_ptr(), sp)
 
     barrier = group.barrier
@@ -699,37 +899,41 @@ def main():
     for _ in range(args.warmup):
         step_device()
     barrier()
-    launches_per_step = ob.last_launch_count()
 
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    # ---- value: device-timed batched steps
+    # ---- value: device-timed batched steps; every step records its stage
+    # events (ovb_two_stage_profile: the same pipeline plus CUDA events between
+    # the stages on the launching stream), so the dominant kernel's launch time
+    # is measured inside the timed region
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    stage_rows = []
     barrier()
     for s in range(args.steps):
         flush.fill_(s & 0xFF)
         ev[s][0].record(stream)
-        step_device()
+        stage_rows.append(ob.two_stage_profile(rq, bm, d_q.data_ptr(), NQ, M, K, d_s.data_ptr(), d_i.data_ptr(), sp))
         ev[s][1].record(stream)
     barrier()
+    launches_per_step = ob.last_launch_count()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = max_over_ranks(sum(step_ms))
     batched_ids = d_i.view(NQ, K).cpu().numpy()
+    batched_scores = d_s.view(NQ, K).cpu().numpy()
+    stages = [statistics.mean(r[j] for r in stage_rows) for j in range(6)]
 
     # ---- e2e: public C ABI, pinned host buffers, H2D + D2H inside the timed region
     h_q = torch.from_numpy(queries).pin_memory()
     h_s = torch.empty(NQ * K, dtype=torch.float32).pin_memory()
     h_i = torch.empty(NQ * K, dtype=torch.int64).pin_memory()
     e2e_ms = []
-    # at least 100 calls: a host-side stall (a clock sample taken while a call
-    # waits on the driver) then weighs about 1 % instead of a tenth of the window
-    e2e_steps = max(args.steps, 100)
+    e2e_steps = max(args.steps, 30)
     for s in range(args.warmup + e2e_steps):
         flush.fill_(s & 0xFF)
         barrier()
         t0 = time.perf_counter()
-        check(lib().ovb_two_stage_search(rq.handle, fs.handle, C.c_void_p(h_q.data_ptr()), NQ, M, K,
+        check(lib().ovb_two_stage_search(rq.handle, bm.handle, C.c_void_p(h_q.data_ptr()), NQ, M, K,
                                          C.c_void_p(h_s.data_ptr()), C.c_void_p(h_i.data_ptr())))
         dt = (time.perf_counter() - t0) * 1e3
         if s >= args.warmup:
@@ -737,7 +941,7 @@ def main():
     e2e_total = max_over_ranks(sum(e2e_ms))
     e2e_same = bool(np.array_equal(h_i.numpy().reshape(NQ, K), batched_ids))
 
-    # ---- plain: one query per launch
+    # ---- plain: one query per call
     P = min(args.plain_queries, NQ)
     pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(P)]
     p_s = torch.empty(P * K, dtype=torch.float32, device=dev)
@@ -754,49 +958,41 @@ def main():
     plain_ms = [a.elapsed_time(b) for a, b in pev]
     plain_launches = ob.last_launch_count()
     identical = bool(np.array_equal(p_i.view(P, K).cpu().numpy(), batched_ids[:P]))
-    serving = serving_run(ob, rq, fs, queries, batched_ids, args.serve_seconds, args.serve_rate) \
-        if args.serve_seconds > 0 else None
+    stages1 = ob.two_stage_profile(rq, bm, d_q.data_ptr(), 1, M, K, p_s.data_ptr(), p_i.data_ptr(), sp)
+    multibucket = second_stage1_run(ob, torch, dev, rq, mb, "MultiBucketBitmap b=2 (diagonal weights)", 4 * QPV,
+                                    d_q, queries, args.plain_queries) if mb is not None else None
     clock_info = clocks.stop()
 
-    # ---- stage profile (roofline of the dominant kernel)
-    flush.fill_(1)
-    barrier()
-    stages = ob.two_stage_profile(rq, fs, d_q.data_ptr(), NQ, M, K, d_s.data_ptr(), d_i.data_ptr(), sp)
-    flush.fill_(2)
-    barrier()
-    stages1 = ob.two_stage_profile(rq, fs, d_q.data_ptr(), 1, M, K, d_s.data_ptr(), d_i.data_ptr(), sp)
-
     hbm_peak, bf16_peak, peak_kind = measured_peaks()
-    pairs_pad = ((DIM // 2 + 31) // 32) * 32
-    code_bytes = ((N_DOCS + 31) // 32) * 16 * pairs_pad  # device layout, read once per launch
-    ref_code_bytes = ((N_DOCS + 31) // 32) * (DIM // 2) * 32
+    code_bytes = N_DOCS * QPV * 8
 
-    def scan_bytes(nq):  # codes once + per-query LUTs + the key row written per query
-        return code_bytes + nq * pairs_pad * 16 + nq * N_DOCS * 4
+    def roof_batched(ms):
+        """bitmap_pair_kernel: the overlap popcount(q AND d) of every (doc,
+        query) pair as an exact u8 GEMM on tcgen05 (kind::i8), A = each doc's
+        768 bits as 0/1 bytes (built in shared memory), B = the queries' bits
+        as 0/1 bytes.  Algorithmic ops = 2 * docs * queries * 768; peak = 2 x
+        the measured dense bf16 rate (kind::i8 issues twice the MACs of
+        kind::f16)."""
+        ops = 2 * N_DOCS * NQ * QPV * 64
+        achieved = ops / (ms * 1e-3) / 1e12
+        return {"bound": "tensor", "achieved": achieved, "peak": 2 * bf16_peak, "unit": "TOPS (int8)",
+                "frac": achieved / (2 * bf16_peak), "traffic": PAIR_FILTER_DRAM_BYTES,
+                "traffic_unit": "DRAM bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
+                "algorithmic_hbm_bytes_per_launch": code_bytes + NQ * QPV * 64,
+                "codes_gbs": code_bytes / (ms * 1e-3) / 1e9,
+                "kernel": "bitmap_pair_kernel (filter epilogue)", "queries_per_launch": NQ,
+                "algorithmic_ops_per_launch": ops, "launch_ms": ms, "launches_timed": len(stage_rows),
+                "timing": "mean of the scan-stage CUDA events of every timed step (launching stream)",
+                "peak_source": f"2 x {peak_kind} bf16 dense TFLOP/s (burst)"}
 
     def roof_plain(ms):
-        """One query: fastscan_scan_kernel (CUDA cores), bound by HBM."""
-        achieved = scan_bytes(1) / (ms * 1e-3) / 1e9
+        """One query: popc_rows_kernel (CUDA cores), bound by HBM: the codes
+        once plus the 4-byte key row."""
+        b = code_bytes + N_DOCS * 4
+        achieved = b / (ms * 1e-3) / 1e9
         return {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                "traffic": None, "kernel": "fastscan_scan_kernel", "queries_per_launch": 1,
-                "algorithmic_bytes_per_launch": scan_bytes(1), "launch_ms": ms,
-                "peak_source": f"{peak_kind} HBM copy bandwidth"}
-
-    def roof_batched(nq, ms):
-        """Batched: fastscan_tc_kernel, the one-hot u8 GEMM on tcgen05 (kind::i8).
-        Algorithmic ops = 2 * docs * queries * K, K = 16 one-hot bytes per
-        nibble pair; peak = 2x the measured dense bf16 rate (kind::i8 issues
-        twice the MACs of kind::f16 per cycle)."""
-        ops = 2 * N_DOCS * nq * pairs_pad * 16
-        achieved = ops / (ms * 1e-3) / 1e12
-        peak = 2 * bf16_peak
-        return {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS (int8)",
-                "frac": achieved / peak, "traffic": TC_FILTER_DRAM_BYTES,
-                "traffic_unit": "DRAM bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
-                "algorithmic_hbm_bytes_per_launch": code_bytes + nq * pairs_pad * 16,
-                "kernel": "fastscan_persist_kernel (filter epilogue)",
-                "queries_per_launch": nq, "algorithmic_ops_per_launch": ops, "launch_ms": ms,
-                "peak_source": f"2 x {peak_kind} bf16 dense TFLOP/s (burst)"}
+                "kernel": "popc_rows_kernel", "queries_per_launch": 1, "algorithmic_bytes_per_launch": b,
+                "launch_ms": ms, "peak_source": f"{peak_kind} HBM copy bandwidth"}
 
     value = whole_job_rate(NQ * args.steps, world, total_ms)
     e2e = whole_job_rate(NQ * e2e_steps, world, e2e_total)
@@ -804,39 +1000,51 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u8-lut/u32-acc/f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_docs": N_DOCS, "dim": DIM, "queries_per_step_per_gpu": NQ, "k": K,
-                   "candidates": M, "form": "batched (one fused two-stage call per step)",
-                   "l2": "flushed between steps by a 256 MiB device write (outside the timed region)",
-                   "parallelism": f"replicas x{world} (queries sharded per rank, no data-path collective)"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8-bits/s32-acc + f64 rerank", "data": "synthetic",
+        "config": headline_config(world),
         "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": NQ * DIM * 4,
                 "d2h_bytes_per_step": NQ * K * (4 + 8), "ms_per_step": e2e_total / e2e_steps, "steps": e2e_steps,
-                "top10_equal_to_device_path": e2e_same},
+                "call": "ovb_two_stage_search (C ABI, pinned host buffers)",
+                "top100_equal_to_device_path": e2e_same},
         "gpu_launches": launches_per_step * args.steps,
         "plain": {"qps": plain_qps, "p50_ms": float(np.percentile(plain_ms, 50)),
                   "p99_ms": float(np.percentile(plain_ms, 99)), "queries": P, "launches_per_query": plain_launches,
-                  "identical_top10_vs_batched": identical, "batched_over_plain": value / world / plain_qps},
-        "serving": serving,
-        "mixed_batch": mixed_run(ob, mixed_q, args.steps) if mixed_q > 0 else None,
-        "sign_b1_plain": sign_plain_run(ob, torch, dev, args.plain_queries, not args.no_cpu) if world == 1 else None,
-        "serving_multi": serving_multi_run(ob, args.serve_seconds, [20_000.0, 100_000.0, args.serve_rate])
-        if world == 1 and args.serve_seconds > 0 else None,
-        "rank_modes": rank_modes_run(ob, torch, dev, rq, queries, args.plain_queries) if world == 1 else None,
-        "large_corpus": large_run(ob, torch, dev, args.steps, args.plain_queries)
-        if args.large == "on" or (args.large == "auto" and world == 1) else None,
+                  "identical_top100_vs_batched": identical, "batched_over_plain": value / world / plain_qps},
         "stages_ms": dict(zip(STAGES, stages)),
         "stages_ms_plain": dict(zip(STAGES, stages1)),
-        "scan_gbs_effective": NQ * ref_code_bytes / (stages[2] * 1e-3) / 1e9,
-        "roofline": roof_batched(NQ, stages[2]),
+        "roofline": roof_batched(stages[2]),
         "roofline_plain": roof_plain(stages1[2]),
+        "multibucket": multibucket,
+        "build_s": build_s,
         "clocks": clock_info,
     }
-    if rank == 0 and not args.no_cpu:
-        qps, threads, sample, _, _, _, qps1 = cpu_two_stage_qps(docs, queries, args.cpu_seconds)
-        line["cpu_baseline"] = {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
+    if cpu:
+        line["codes_identical_to_oracle"] = bool(np.array_equal(bm.payload().view(np.uint64), h_words)
+                                                 and np.array_equal(rq.payload(), h_packed))
+        threads = orc.max_threads()
+        run = lambda qs: orc.cpu_bitmap_two_stage(h_words, h_packed, N_DOCS, DIM, N_TOP, BITS, qs, M, K, threads)
+        probe = min(NQ, 8 * threads)
+        t0 = time.perf_counter()
+        run(queries[:probe])
+        probe_qps = probe / (time.perf_counter() - t0)
+        sample = cpu_sample_size(probe_qps, args.cpu_seconds, 8, NQ)
+        t0 = time.perf_counter()
+        cs, ci = run(queries[:sample])
+        dt = time.perf_counter() - t0
+        same, tol_same, rows = topk_agreement(orc, h_packed, DIM, BITS, queries[:sample], batched_ids[:sample], ci)
+        line["cpu_baseline"] = {"value": sample / dt, "unit": "queries/s", "cores": threads, "kind": "port",
                                 "sample": f"first {sample} of the step's {NQ} queries, all host threads",
-                                "value_1thread": qps1, "sample_1thread": "first 16 queries, one thread",
-                                "cpu_model": cpu_model()}
+                                "cpu_model": cpu_model(), "identical_top100_vs_cpu": same,
+                                "equal_up_to_fp64_near_ties": tol_same, "rows_differing": rows}
+        line["identical_top100_vs_cpu"] = same
+    if extras:
+        del mb, multibucket
+        line["fastscan_two_stage"] = fastscan_run(ob, torch, dev, args, cpu)
+        line["mixed_batch"] = mixed_run(ob, mixed_q, args.steps) if mixed_q > 0 else None
+        line["sign_b1_plain"] = sign_plain_run(ob, torch, dev, args.plain_queries, cpu)
+        line["serving_multi"] = serving_multi_run(ob, args.serve_seconds, [20_000.0, 100_000.0, args.serve_rate]) \
+            if args.serve_seconds > 0 else None
+        line["rank_modes"] = rank_modes_run(ob, torch, dev, args.plain_queries)
     group.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

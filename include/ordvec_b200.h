@@ -311,7 +311,11 @@ ordvec_status_t ovb_two_stage_profile(const ordvec_index_t *rq, const ordvec_ind
  * it): requests needing more (nq*dim*4 + nq*n*4 + 2*nq*k*4 bytes, each part
  * rounded up to 256) or k > 4096 are rejected with BAD_ARGUMENT.  The first
  * call on a device looks up the array's device address; make it before any
- * stream capture.  Calls that overlap on the GPU share the array and race. */
+ * stream capture, and do not use the entry point across a cudaDeviceReset
+ * (the cached address would be stale).  Calls that overlap on the GPU share
+ * the array and race.  Queries must be finite: they are not checked (that
+ * would need a device-to-host read), and a non-finite query's ranking is
+ * unspecified. */
 ordvec_status_t ovb_rankquant_search_noalloc(const ordvec_index_t *rq, const float *d_queries,
                                              uint64_t nq, uint64_t k, float *d_scores,
                                              int64_t *d_ids, void *stream);

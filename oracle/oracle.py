@@ -74,9 +74,14 @@ _SIGS = {
     "orc_xorshift_f32": (None, [U64, U64, f32p]),
     "orc_avx512_available": (I, []),
     "orc_max_threads": (I, []),
-    "orc_cpu_fastscan_two_stage": (None, [u8p, u8p, U64, U32, f32p, U64, U64, U64, I, f32p, i64p]),
+    "orc_cpu_fastscan_two_stage": (None, [u8p, u8p, U64, U32, f32p, U64, U64, U64, I, f32p, i64p, C.c_void_p]),
     "orc_cpu_sign_two_stage": (None, [u64p, u8p, U64, U32, U32, f32p, U64, U64, U64, I, f32p, i64p]),
     "orc_cpu_rq_search_asym": (None, [u8p, U64, U32, U32, f32p, U64, U64, I, f32p, i64p]),
+    "orc_cpu_bitmap_two_stage": (None, [u64p, u8p, U64, U32, U32, U32, f32p, U64, U64, U64, I, f32p, i64p,
+                                        C.c_void_p]),
+    "orc_synth_docs": (None, [U64, U64, U64, U32, F32, f32p]),
+    "orc_synth_queries": (None, [U64, U64, U64, U32, F32, F32, f32p, u64p]),
+    "orc_encode_bitmap_rankquant": (None, [f32p, U64, U32, U32, U32, C.c_void_p, C.c_void_p]),
 }
 
 
@@ -419,14 +424,23 @@ def xorshift_f32(seed, count):
 
 
 # ---- timed CPU baseline (AVX-512 + OpenMP restatement) -------------------------
-def cpu_fastscan_two_stage(blocks, packed_b2, n, dim, queries, n_candidates, k, threads):
+def cpu_fastscan_two_stage(blocks, packed_b2, n, dim, queries, n_candidates, k, threads, want_candidates=False):
+    """FastScan top-n_candidates -> RankQuant b=2 subset rerank, parallel over
+    queries.  Returns (scores, ids) nq x min(k, n_candidates, n) and, with
+    want_candidates, the nq x min(n_candidates, n) candidate rows."""
     q, nq = _rows(queries, dim)
-    out_k = min(k, n_candidates, n)
+    cand = min(n_candidates, n)
+    out_k = min(k, cand)
     s = np.empty(nq * out_k, np.float32)
     i = np.empty(nq * out_k, np.int64)
+    cands = np.empty(max(nq * cand, 1), np.uint32) if want_candidates else None
     lib().orc_cpu_fastscan_two_stage(np.ascontiguousarray(blocks, np.uint8), np.ascontiguousarray(packed_b2, np.uint8),
-                                     n, dim, q, nq, n_candidates, k, threads, s, i)
-    return s.reshape(nq, out_k), i.reshape(nq, out_k)
+                                     n, dim, q, nq, n_candidates, k, threads, s, i,
+                                     cands.ctypes.data if cands is not None else None)
+    out = (s.reshape(nq, out_k), i.reshape(nq, out_k))
+    if want_candidates:
+        return out + (cands[: nq * cand].reshape(nq, cand),)
+    return out
 
 
 def cpu_sign_two_stage(sign_words, packed, n, dim, bits, queries, m, k, threads):
@@ -446,6 +460,57 @@ def cpu_rq_search_asym(packed, n, dim, bits, queries, k, threads):
     i = np.empty(nq * ke, np.int64)
     lib().orc_cpu_rq_search_asym(np.ascontiguousarray(packed, np.uint8), n, dim, bits, q, nq, k, threads, s, i)
     return s.reshape(nq, ke), i.reshape(nq, ke)
+
+
+def cpu_bitmap_two_stage(words, packed, n, dim, n_top, bits, queries, m, k, threads, want_candidates=False):
+    """Bitmap top-m (batched chunks of 8 queries, AVX-512) -> RankQuant subset
+    rerank, parallel over query groups.  Returns (scores, ids) nq x min(k, m, n)
+    and, with want_candidates, the nq x min(m, n) candidate rows."""
+    q, nq = _rows(queries, dim)
+    me = min(m, n)
+    out_k = min(k, me)
+    s = np.empty(max(nq * out_k, 1), np.float32)
+    i = np.empty(max(nq * out_k, 1), np.int64)
+    cands = np.empty(max(nq * me, 1), np.uint32) if want_candidates else None
+    lib().orc_cpu_bitmap_two_stage(np.ascontiguousarray(words, np.uint64), np.ascontiguousarray(packed, np.uint8),
+                                   n, dim, n_top, bits, q, nq, m, k, threads, s, i,
+                                   cands.ctypes.data if cands is not None else None)
+    out = (s[: nq * out_k].reshape(nq, out_k), i[: nq * out_k].reshape(nq, out_k))
+    if want_candidates:
+        return out + (cands[: nq * me].reshape(nq, me),)
+    return out
+
+
+# ---- benchmark corpus (the seeded clustered-Gaussian generator) ------------------
+DOC_SIGMA, QUERY_SIGMA = 0.3, 0.1
+
+
+def synth_docs(seed, n, dim, sigma=DOC_SIGMA, first=0):
+    """Rows first .. first+n-1 of the benchmark corpus (n x dim float32)."""
+    out = np.empty((n, dim), np.float32)
+    lib().orc_synth_docs(seed, first, n, dim, sigma, out.reshape(-1))
+    return out
+
+
+def synth_queries(seed, n_docs, nq, dim, doc_sigma=DOC_SIGMA, query_sigma=QUERY_SIGMA):
+    """(queries nq x dim float32, planted source doc ids)."""
+    out = np.empty((nq, dim), np.float32)
+    planted = np.empty(nq, np.uint64)
+    lib().orc_synth_queries(seed, n_docs, nq, dim, doc_sigma, query_sigma, out.reshape(-1), planted)
+    return out, planted
+
+
+def encode_bitmap_rankquant(vecs, dim, n_top, bits, bitmap_out=None, rq_out=None):
+    """One rank transform per row, both layouts written (each output optional):
+    the bytes of bitmap_encode and rankquant_encode."""
+    v, n = _rows(vecs, dim)
+    if bitmap_out is not None:
+        assert bitmap_out.dtype == np.uint64 and bitmap_out.flags.c_contiguous and bitmap_out.size == n * (dim // 64)
+    if rq_out is not None:
+        assert rq_out.dtype == np.uint8 and rq_out.flags.c_contiguous and rq_out.size == n * dim * bits // 8
+    lib().orc_encode_bitmap_rankquant(v, n, dim, n_top, bits,
+                                      bitmap_out.ctypes.data if bitmap_out is not None else None,
+                                      rq_out.ctypes.data if rq_out is not None else None)
 
 
 def avx512_available():

@@ -39,14 +39,6 @@ static inline int total_cmp(float a, float b) {
 
 typedef struct { float v; uint32_t i; } vi_t;
 
-/* cmp_finite_f32_then_index (src/util.rs:19-30): equal values (== , so
- * -0.0 == +0.0) order by index, otherwise by total_cmp. */
-static int cmp_rank(const void *pa, const void *pb) {
-    const vi_t *a = (const vi_t *)pa, *b = (const vi_t *)pb;
-    if (a->v == b->v) return (a->i > b->i) - (a->i < b->i);
-    return total_cmp(a->v, b->v);
-}
-
 static int cmp_u64(const void *pa, const void *pb) {
     uint64_t a = *(const uint64_t *)pa, b = *(const uint64_t *)pb;
     return (a > b) - (a < b);
@@ -57,13 +49,41 @@ static int cmp_u64(const void *pa, const void *pb) {
 /* ------------------------------------------------------------------ */
 
 /* rank_transform (src/rank.rs:38-53): argsort with the index tiebreak,
- * then invert the permutation. */
+ * then invert the permutation.  The order of cmp_finite_f32_then_index
+ * (src/util.rs:19-30: values equal under ==, so -0.0 == +0.0, tie by index,
+ * otherwise total_cmp) is the unsigned order of the
+ * total_cmp key with -0.0 folded onto +0.0, broken by index; a stable LSD
+ * radix sort over that 32-bit key, fed in index order, produces it without
+ * a comparison callback (the 10M-row benchmark corpora are encoded on the
+ * host with it).  NaN inputs, which the reference rejects, are ordered by
+ * their bit patterns. */
 void orc_rank_transform(const float *v, uint32_t d, uint16_t *out) {
-    vi_t *o = (vi_t *)malloc(sizeof(vi_t) * (d ? d : 1));
-    for (uint32_t i = 0; i < d; i++) { o[i].v = v[i]; o[i].i = i; }
-    qsort(o, d, sizeof(vi_t), cmp_rank);
-    for (uint32_t r = 0; r < d; r++) out[o[r].i] = (uint16_t)r;
-    free(o);
+    if (d == 0) return;
+    uint32_t *key = (uint32_t *)malloc(4 * (size_t)d * 2);
+    uint16_t *idx = (uint16_t *)malloc(2 * (size_t)d * 2);
+    uint32_t *k2 = key + d;
+    uint16_t *i2 = idx + d;
+    for (uint32_t i = 0; i < d; i++) {
+        float f = v[i] == 0.0f ? 0.0f : v[i];
+        key[i] = (uint32_t)total_key(f) ^ 0x80000000u;
+        idx[i] = (uint16_t)i;
+    }
+    for (int pass = 0; pass < 4; pass++) {
+        uint32_t shift = 8u * (uint32_t)pass, cnt[257] = {0};
+        for (uint32_t i = 0; i < d; i++) cnt[((key[i] >> shift) & 0xFF) + 1]++;
+        if (cnt[((key[0] >> shift) & 0xFF) + 1] == d) continue; /* one digit value: order unchanged */
+        for (int b = 0; b < 256; b++) cnt[b + 1] += cnt[b];
+        for (uint32_t i = 0; i < d; i++) {
+            uint32_t p = cnt[(key[i] >> shift) & 0xFF]++;
+            k2[p] = key[i];
+            i2[p] = idx[i];
+        }
+        uint32_t *tk = key; key = k2; k2 = tk;
+        uint16_t *ti = idx; idx = i2; i2 = ti;
+    }
+    for (uint32_t r = 0; r < d; r++) out[idx[r]] = (uint16_t)r;
+    free(key < k2 ? key : k2);
+    free(idx < i2 ? idx : i2);
 }
 
 /* rank_to_bucket (src/rank.rs:89-95): floor(rank * 2^bits / d) in u64. */
@@ -995,6 +1015,163 @@ void orc_xorshift_f32(uint64_t seed, uint64_t count, float *out) {
 }
 
 /* ------------------------------------------------------------------ */
+/* benchmark corpus generator                                         */
+/* ------------------------------------------------------------------ */
+
+/* The seeded clustered-Gaussian corpus of the benchmark configurations,
+ * restated here so the CPU legs of the benchmark build their inputs without
+ * the product library: 256 clusters, centre = N(0, I) normalised to unit
+ * norm, doc = centre[cluster] + N(0, sigma^2) per coordinate, L2-normalised
+ * in f64 and stored as f32; a query is a uniformly chosen doc plus
+ * N(0, query_sigma^2), renormalised.  Every row owns a xoshiro256** stream
+ * seeded through SplitMix64 from (seed, tag, row) -- tag 1 centres, 2 docs,
+ * 3 queries (whose stream uses seed + 1) -- and normals come from
+ * Box-Muller in f64, so any row range is reproducible on its own. */
+typedef struct { uint64_t s[4]; } synth_rng;
+
+static uint64_t synth_splitmix(uint64_t *x) {
+    uint64_t z = (*x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static void synth_seed(synth_rng *r, uint64_t seed, uint64_t tag, uint64_t row) {
+    uint64_t x = seed ^ (tag * 0xD1B54A32D192ED03ull) ^ (row * 0x8CB92BA72F3D8DD7ull);
+    for (int i = 0; i < 4; i++) r->s[i] = synth_splitmix(&x);
+}
+
+static inline uint64_t synth_rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+
+static uint64_t synth_next(synth_rng *r) {
+    uint64_t *s = r->s;
+    const uint64_t out = synth_rotl(s[1] * 5, 7) * 9, t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = synth_rotl(s[3], 45);
+    return out;
+}
+
+static double synth_uniform(synth_rng *r) { return (double)(synth_next(r) >> 11) * 0x1.0p-53; }
+
+static void synth_normals(synth_rng *r, double *out, uint32_t n) {
+    for (uint32_t i = 0; i < n; i += 2) {
+        const double u1 = 1.0 - synth_uniform(r), u2 = synth_uniform(r);
+        const double rad = sqrt(-2.0 * log(u1)), a = 6.283185307179586 * u2;
+        out[i] = rad * cos(a);
+        if (i + 1 < n) out[i + 1] = rad * sin(a);
+    }
+}
+
+static void synth_normalise(double *v, uint32_t dim) {
+    double s = 0.0;
+    for (uint32_t j = 0; j < dim; j++) s += v[j] * v[j];
+    const double inv = s > 0.0 ? 1.0 / sqrt(s) : 0.0;
+    for (uint32_t j = 0; j < dim; j++) v[j] *= inv;
+}
+
+#define SYNTH_CLUSTERS 256u
+
+static double *synth_centres(uint64_t seed, uint32_t dim) {
+    double *c = (double *)malloc(sizeof(double) * SYNTH_CLUSTERS * dim + 8);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < (int)SYNTH_CLUSTERS; k++) {
+        synth_rng r;
+        synth_seed(&r, seed, 1, (uint64_t)k);
+        synth_normals(&r, c + (size_t)k * dim, dim);
+        synth_normalise(c + (size_t)k * dim, dim);
+    }
+    return c;
+}
+
+static void synth_doc_row(uint64_t seed, uint64_t row, uint32_t dim, double sigma, const double *cen,
+                          double *tmp, float *out) {
+    synth_rng r;
+    synth_seed(&r, seed, 2, row);
+    const uint32_t cl = (uint32_t)(synth_next(&r) >> 56);
+    synth_normals(&r, tmp, dim);
+    const double *c = cen + (size_t)cl * dim;
+    for (uint32_t j = 0; j < dim; j++) tmp[j] = c[j] + sigma * tmp[j];
+    synth_normalise(tmp, dim);
+    for (uint32_t j = 0; j < dim; j++) out[j] = (float)tmp[j];
+}
+
+void orc_synth_docs(uint64_t seed, uint64_t first, uint64_t n, uint32_t dim, float sigma, float *out) {
+    if (dim == 0 || n == 0) return;
+    double *cen = synth_centres(seed, dim);
+#pragma omp parallel
+    {
+        double *tmp = (double *)malloc(sizeof(double) * (dim + 1));
+#pragma omp for schedule(static)
+        for (int64_t i = 0; i < (int64_t)n; i++)
+            synth_doc_row(seed, first + (uint64_t)i, dim, sigma, cen, tmp, out + (uint64_t)i * dim);
+        free(tmp);
+    }
+    free(cen);
+}
+
+void orc_synth_queries(uint64_t seed, uint64_t n_docs, uint64_t nq, uint32_t dim, float doc_sigma,
+                       float query_sigma, float *out, uint64_t *planted) {
+    if (dim == 0 || nq == 0 || n_docs == 0) return;
+    double *cen = synth_centres(seed, dim);
+#pragma omp parallel
+    {
+        double *tmp = (double *)malloc(sizeof(double) * (dim + 1));
+        double *noise = (double *)malloc(sizeof(double) * (dim + 1));
+        float *doc = (float *)malloc(sizeof(float) * dim);
+#pragma omp for schedule(static)
+        for (int64_t i = 0; i < (int64_t)nq; i++) {
+            synth_rng r;
+            synth_seed(&r, seed + 1, 3, (uint64_t)i);
+            const uint64_t src = (uint64_t)(((unsigned __int128)synth_next(&r) * n_docs) >> 64);
+            synth_doc_row(seed, src, dim, doc_sigma, cen, tmp, doc);
+            synth_normals(&r, noise, dim);
+            for (uint32_t j = 0; j < dim; j++) tmp[j] = (double)doc[j] + query_sigma * noise[j];
+            synth_normalise(tmp, dim);
+            for (uint32_t j = 0; j < dim; j++) out[(uint64_t)i * dim + j] = (float)tmp[j];
+            if (planted) planted[i] = src;
+        }
+        free(tmp);
+        free(noise);
+        free(doc);
+    }
+    free(cen);
+}
+
+/* Bitmap::add and RankQuant::add in one pass over the rows (one rank
+ * transform per row, shared by both layouts): the same bytes as
+ * orc_bitmap_encode and orc_rankquant_encode.  Either output may be NULL. */
+void orc_encode_bitmap_rankquant(const float *vecs, uint64_t n, uint32_t dim, uint32_t n_top,
+                                 uint32_t bits, uint64_t *bitmap_out, uint8_t *rq_out) {
+    uint32_t qpv = dim / 64, bpv = dim * bits / 8;
+    uint16_t cutoff = (uint16_t)(dim - n_top);
+#pragma omp parallel
+    {
+        uint16_t *r = (uint16_t *)malloc(2 * dim);
+        uint8_t *b = (uint8_t *)malloc(dim);
+#pragma omp for schedule(static)
+        for (int64_t i = 0; i < (int64_t)n; i++) {
+            orc_rank_transform(vecs + (uint64_t)i * dim, dim, r);
+            if (bitmap_out) {
+                uint64_t *row = bitmap_out + (uint64_t)i * qpv;
+                memset(row, 0, 8 * (size_t)qpv);
+                for (uint32_t j = 0; j < dim; j++)
+                    if (r[j] >= cutoff) row[j / 64] |= (uint64_t)1 << (j % 64);
+            }
+            if (rq_out) {
+                for (uint32_t j = 0; j < dim; j++) b[j] = (uint8_t)orc_rank_to_bucket(r[j], dim, bits);
+                orc_pack_buckets(b, dim, bits, rq_out + (uint64_t)i * bpv);
+            }
+        }
+        free(r);
+        free(b);
+    }
+}
+
+/* ------------------------------------------------------------------ */
 /* AVX-512 + OpenMP restatement (timed CPU baseline only)             */
 /* ------------------------------------------------------------------ */
 
@@ -1174,11 +1351,13 @@ static void cpu_subset_row(const uint8_t *packed, uint32_t dim, uint32_t bits, c
 
 /* RankQuantFastscan::search(q, n_candidates) -> RankQuant b=2
  * search_asymmetric_subset(q, ids, k) per query, parallel over queries the
- * way rayon's par_chunks is (src/fastscan.rs:430-468, src/quant.rs:1048). */
+ * way rayon's par_chunks is (src/fastscan.rs:430-468, src/quant.rs:1048).
+ * `cands_out` (nq x min(n_candidates, n), may be NULL) receives each query's
+ * FastScan candidate row in TopK order. */
 void orc_cpu_fastscan_two_stage(const uint8_t *blocks, const uint8_t *packed_b2, uint64_t n,
                                 uint32_t dim, const float *queries, uint64_t nq,
                                 uint64_t n_candidates, uint64_t k, int nthreads,
-                                float *scores, int64_t *ids) {
+                                float *scores, int64_t *ids, uint32_t *cands_out) {
     uint64_t cand = n_candidates < n ? n_candidates : n;
     uint64_t out_k = k < cand ? k : cand;
     float inv_norm = 1.0f / orc_rankquant_norm(dim, 2);
@@ -1205,6 +1384,7 @@ void orc_cpu_fastscan_two_stage(const uint8_t *blocks, const uint8_t *packed_b2,
             orc_topk_finalize(t, cs, ci, cand);
             orc_topk_free(t);
             for (uint64_t i = 0; i < cand; i++) cu[i] = (uint32_t)ci[i];
+            if (cands_out) memcpy(cands_out + (uint64_t)qi * cand, cu, 4 * cand);
             cpu_subset_row(packed_b2, dim, 2, qu, cu, cand, out_k, scratch,
                            scores + (uint64_t)qi * out_k, ids + (uint64_t)qi * out_k);
             free(qu);
@@ -1253,6 +1433,125 @@ void orc_cpu_sign_two_stage(const uint64_t *sign_words, const uint8_t *packed, u
             free(qu);
         }
         free(h); free(key); free(qb); free(cu); free(scratch);
+    }
+}
+
+/* bitmap_scan_collect_batched_avx512vpop (src/bitmap.rs:813-936): the doc
+ * stream is read once per group of CHUNK = 8 queries; each doc's words are
+ * ANDed with the group's query words, VPOPCNTQ'd and summed per query, the
+ * trailing qpv % 8 words through a masked load; a final group of fewer
+ * than 8 queries runs the same loop with a runtime bound. */
+#define BITMAP_BATCH_CHUNK 8
+AVX512 static void bitmap_batched_avx512(const uint64_t *words, uint64_t n, uint32_t qpv,
+                                         const uint64_t *qb, uint32_t batch, uint32_t *scores) {
+    uint32_t lanes = qpv / 8, rem = qpv % 8;
+    __mmask8 tm = rem ? (__mmask8)((1u << rem) - 1) : 0;
+    __m512i *qz = (__m512i *)aligned_alloc(64, 64 * ((size_t)batch * (lanes + 1) + 1));
+    for (uint32_t b = 0; b < batch; b++) {
+        for (uint32_t l = 0; l < lanes; l++) qz[b * (lanes + 1) + l] = _mm512_loadu_si512(qb + (uint64_t)b * qpv + l * 8);
+        qz[b * (lanes + 1) + lanes] = rem ? _mm512_maskz_loadu_epi64(tm, qb + (uint64_t)b * qpv + lanes * 8)
+                                          : _mm512_setzero_si512();
+    }
+    uint32_t start = 0;
+    for (; start + BITMAP_BATCH_CHUNK <= batch; start += BITMAP_BATCH_CHUNK) {
+        for (uint64_t di = 0; di < n; di++) {
+            const uint64_t *d = words + di * qpv;
+            __m512i acc[BITMAP_BATCH_CHUNK];
+            for (int b = 0; b < BITMAP_BATCH_CHUNK; b++) acc[b] = _mm512_setzero_si512();
+            for (uint32_t l = 0; l < lanes; l++) {
+                __m512i dz = _mm512_loadu_si512(d + l * 8);
+                for (int b = 0; b < BITMAP_BATCH_CHUNK; b++)
+                    acc[b] = _mm512_add_epi64(acc[b], _mm512_popcnt_epi64(_mm512_and_si512(dz, qz[(start + b) * (lanes + 1) + l])));
+            }
+            if (rem) {
+                __m512i dz = _mm512_maskz_loadu_epi64(tm, d + lanes * 8);
+                for (int b = 0; b < BITMAP_BATCH_CHUNK; b++)
+                    acc[b] = _mm512_add_epi64(acc[b], _mm512_popcnt_epi64(_mm512_and_si512(dz, qz[(start + b) * (lanes + 1) + lanes])));
+            }
+            for (int b = 0; b < BITMAP_BATCH_CHUNK; b++)
+                scores[(uint64_t)(start + b) * n + di] = (uint32_t)_mm512_reduce_add_epi64(acc[b]);
+        }
+    }
+    uint32_t tail = batch - start;
+    if (tail) {
+        for (uint64_t di = 0; di < n; di++) {
+            const uint64_t *d = words + di * qpv;
+            __m512i acc[BITMAP_BATCH_CHUNK];
+            for (uint32_t b = 0; b < tail; b++) acc[b] = _mm512_setzero_si512();
+            for (uint32_t l = 0; l < lanes; l++) {
+                __m512i dz = _mm512_loadu_si512(d + l * 8);
+                for (uint32_t b = 0; b < tail; b++)
+                    acc[b] = _mm512_add_epi64(acc[b], _mm512_popcnt_epi64(_mm512_and_si512(dz, qz[(start + b) * (lanes + 1) + l])));
+            }
+            if (rem) {
+                __m512i dz = _mm512_maskz_loadu_epi64(tm, d + lanes * 8);
+                for (uint32_t b = 0; b < tail; b++)
+                    acc[b] = _mm512_add_epi64(acc[b], _mm512_popcnt_epi64(_mm512_and_si512(dz, qz[(start + b) * (lanes + 1) + lanes])));
+            }
+            for (uint32_t b = 0; b < tail; b++)
+                scores[(uint64_t)(start + b) * n + di] = (uint32_t)_mm512_reduce_add_epi64(acc[b]);
+        }
+    }
+    free(qz);
+}
+
+static void bitmap_batched_scalar(const uint64_t *words, uint64_t n, uint32_t qpv, const uint64_t *qb,
+                                  uint32_t batch, uint32_t *scores) {
+    for (uint64_t di = 0; di < n; di++)
+        for (uint32_t b = 0; b < batch; b++) {
+            uint32_t s = 0;
+            for (uint32_t w = 0; w < qpv; w++)
+                s += (uint32_t)__builtin_popcountll(words[di * qpv + w] & qb[(uint64_t)b * qpv + w]);
+            scores[(uint64_t)b * n + di] = s;
+        }
+}
+
+/* Bitmap::top_m_candidates_batched_chunked(queries, m, 8)
+ * (src/bitmap.rs:304-367, 376-399: groups of 8 queries in parallel, one
+ * batched scan per group, then per query the top-m by (overlap desc, id asc),
+ * sorted) followed by RankQuant::search_asymmetric_subset per query
+ * (src/quant.rs:1048-1083, 1126-1281; AVX-512 centre-drop for b=2/4 at
+ * dim % 64 == 0).  `cands_out` (nq x min(m, n), may be NULL) receives each
+ * query's candidate row. */
+void orc_cpu_bitmap_two_stage(const uint64_t *bitmap_words, const uint8_t *packed, uint64_t n,
+                              uint32_t dim, uint32_t n_top, uint32_t bits, const float *queries,
+                              uint64_t nq, uint64_t m, uint64_t k, int nthreads, float *scores,
+                              int64_t *ids, uint32_t *cands_out) {
+    uint64_t me = m < n ? m : n;
+    uint64_t out_k = k < me ? k : me;
+    if (me == 0 || nq == 0) return;
+    uint32_t qpv = dim / 64;
+    int use_avx = orc_avx512_available();
+    int64_t groups = (int64_t)((nq + BITMAP_BATCH_CHUNK - 1) / BITMAP_BATCH_CHUNK);
+#pragma omp parallel num_threads(nthreads)
+    {
+        uint32_t *sc = (uint32_t *)malloc(4 * n * BITMAP_BATCH_CHUNK);
+        uint64_t *key = (uint64_t *)malloc(8 * n);
+        uint64_t *qb = (uint64_t *)malloc(8 * (size_t)qpv * BITMAP_BATCH_CHUNK);
+        uint32_t *cu = (uint32_t *)malloc(4 * me);
+        uint8_t *scratch = (uint8_t *)malloc(me * (dim * bits / 8));
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t g = 0; g < groups; g++) {
+            uint64_t q0 = (uint64_t)g * BITMAP_BATCH_CHUNK;
+            uint32_t batch = (uint32_t)(nq - q0 < BITMAP_BATCH_CHUNK ? nq - q0 : BITMAP_BATCH_CHUNK);
+            for (uint32_t b = 0; b < batch; b++)
+                orc_bitmap_query_fp32(queries + (q0 + b) * dim, dim, n_top, qb + (uint64_t)b * qpv);
+            if (use_avx) bitmap_batched_avx512(bitmap_words, n, qpv, qb, batch, sc);
+            else bitmap_batched_scalar(bitmap_words, n, qpv, qb, batch, sc);
+            for (uint32_t b = 0; b < batch; b++) {
+                const uint32_t *row = sc + (uint64_t)b * n;
+                for (uint64_t i = 0; i < n; i++) key[i] = ((uint64_t)(UINT32_MAX - row[i]) << 32) | i;
+                select_smallest(key, n, me);
+                qsort(key, me, 8, cmp_u64);
+                for (uint64_t i = 0; i < me; i++) cu[i] = (uint32_t)key[i];
+                uint64_t qi = q0 + b;
+                if (cands_out) memcpy(cands_out + qi * me, cu, 4 * me);
+                float *qu = alloc_unit(queries + qi * dim, dim);
+                cpu_subset_row(packed, dim, bits, qu, cu, me, out_k, scratch, scores + qi * out_k, ids + qi * out_k);
+                free(qu);
+            }
+        }
+        free(sc); free(key); free(qb); free(cu); free(scratch);
     }
 }
 

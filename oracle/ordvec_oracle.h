@@ -127,17 +127,28 @@ uint64_t orc_multibucket_top_m(const uint64_t *words, uint64_t n, uint32_t dim,
 /* ---- test-corpus helper (tests/tiled_candgen.rs XorShift) ---- */
 void orc_xorshift_f32(uint64_t seed, uint64_t count, float *out);
 
+/* ---- benchmark corpus generator and a one-pass host encoder ---- */
+void orc_synth_docs(uint64_t seed, uint64_t first, uint64_t n, uint32_t dim, float sigma, float *out);
+void orc_synth_queries(uint64_t seed, uint64_t n_docs, uint64_t nq, uint32_t dim, float doc_sigma,
+                       float query_sigma, float *out, uint64_t *planted);
+void orc_encode_bitmap_rankquant(const float *vecs, uint64_t n, uint32_t dim, uint32_t n_top,
+                                 uint32_t bits, uint64_t *bitmap_out, uint8_t *rq_out);
+
 /* ---- AVX-512 + OpenMP restatement, used only as the timed CPU baseline ---- */
 int orc_avx512_available(void);
 int orc_max_threads(void);
 void orc_cpu_fastscan_two_stage(const uint8_t *blocks, const uint8_t *packed_b2, uint64_t n,
                                 uint32_t dim, const float *queries, uint64_t nq,
                                 uint64_t n_candidates, uint64_t k, int nthreads,
-                                float *scores, int64_t *ids);
+                                float *scores, int64_t *ids, uint32_t *cands_out);
 void orc_cpu_sign_two_stage(const uint64_t *sign_words, const uint8_t *packed, uint64_t n,
                             uint32_t dim, uint32_t bits, const float *queries, uint64_t nq,
                             uint64_t m, uint64_t k, int nthreads, float *scores,
                             int64_t *ids);
+void orc_cpu_bitmap_two_stage(const uint64_t *bitmap_words, const uint8_t *packed, uint64_t n,
+                              uint32_t dim, uint32_t n_top, uint32_t bits, const float *queries,
+                              uint64_t nq, uint64_t m, uint64_t k, int nthreads, float *scores,
+                              int64_t *ids, uint32_t *cands_out);
 void orc_cpu_rq_search_asym(const uint8_t *packed, uint64_t n, uint32_t dim, uint32_t bits,
                             const float *queries, uint64_t nq, uint64_t k, int nthreads,
                             float *scores, int64_t *ids);

@@ -17,10 +17,18 @@
 // that device is current; the first call on each device does this set-up, so
 // that first call should come before any stream capture.
 //
+// The cached address belongs to the device context it was looked up in: after
+// cudaDeviceReset the next call would reuse a stale address, so this entry
+// point must not be used across a device reset.
+//
 // Every call shares the array and it keeps the last call's contents.  Nothing
 // in it needs to start at zero: each byte a call reads is written earlier in
 // the same call.  Calls whose work overlaps on the GPU (different streams, or
 // different host threads) race on the array; serialise them.
+//
+// Queries are not checked for finiteness here (that check needs a device to
+// host read, i.e. a synchronisation); the caller passes finite queries, and
+// the ranking of a non-finite query is unspecified.
 #include <cmath>
 #include <functional>
 #include <mutex>
@@ -57,6 +65,12 @@ uint8_t* scratch_base() {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// a * b * c in 64 bits, or false when the product does not fit.
+bool mul3(uint64_t a, uint64_t b, uint64_t c, uint64_t* out) {
+  uint64_t ab = 0;
+  return !__builtin_mul_overflow(a, b, &ab) && !__builtin_mul_overflow(ab, c, out);
+}
+
 }  // namespace
 }  // namespace ovb
 
@@ -71,6 +85,7 @@ extern "C" ordvec_status_t ovb_rankquant_search_noalloc(const ordvec_index_t* rq
                                                         uint64_t nq, uint64_t k, float* d_scores,
                                                         int64_t* d_ids, void* stream) {
   return api_boundary([&] {
+    ensure_device();
     const Index& ix = as_index(rq);
     if (ix.kind != ORDVEC_INDEX_KIND_RANK_QUANT)
       fail(ORDVEC_STATUS_UNSUPPORTED_OPERATION, "ovb_rankquant_search_noalloc needs a RankQuant index");
@@ -80,16 +95,22 @@ extern "C" ordvec_status_t ovb_rankquant_search_noalloc(const ordvec_index_t* rq
     if (!d_scores || !d_ids) fail(ORDVEC_STATUS_NULL_POINTER, "output pointer is NULL");
     if (ke > kSelectSmemCap)
       fail(ORDVEC_STATUS_BAD_ARGUMENT, "ovb_rankquant_search_noalloc supports k <= 4096");
-    const size_t q_bytes = align256(nq * ix.dim * 4);
-    const size_t key_bytes = align256(nq * ix.n * 4);
-    const size_t sel_bytes = align256(nq * ke * 4);
+    // each part is checked for 64-bit overflow and against the array size
+    // before it is rounded and summed, so a huge nq cannot wrap the total
+    uint64_t parts[3];
+    const bool fits = mul3(nq, ix.dim, 4, &parts[0]) && mul3(nq, ix.n, 4, &parts[1]) &&
+                      mul3(nq, ke, 4, &parts[2]) && parts[0] <= kNoAllocScratchBytes &&
+                      parts[1] <= kNoAllocScratchBytes && parts[2] <= kNoAllocScratchBytes;
+    const size_t q_bytes = fits ? align256(parts[0]) : 0;
+    const size_t key_bytes = fits ? align256(parts[1]) : 0;
+    const size_t sel_bytes = fits ? align256(parts[2]) : 0;
     const size_t need = q_bytes + key_bytes + 2 * sel_bytes;
-    if (need > kNoAllocScratchBytes)
+    if (!fits || need > kNoAllocScratchBytes)
       fail(ORDVEC_STATUS_BAD_ARGUMENT,
            "ovb_rankquant_search_noalloc: nq=" + std::to_string(nq) + ", n=" + std::to_string(ix.n) + ", k=" +
-               std::to_string(ke) + " needs " + std::to_string(need) +
-               " bytes of scratch; the allocation-free entry point is limited to " +
-               std::to_string(kNoAllocScratchBytes) + " bytes (32 MiB): use ovb_rankquant_search or smaller batches");
+               std::to_string(ke) + " needs more than the " + std::to_string(kNoAllocScratchBytes) +
+               " bytes (32 MiB) of scratch the allocation-free entry point has: use ovb_rankquant_search or "
+               "smaller batches");
     uint8_t* base = scratch_base();
     float* qu = (float*)base;
     uint32_t* keys = (uint32_t*)(base + q_bytes);

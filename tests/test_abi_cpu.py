@@ -140,6 +140,19 @@ def test_synth_generator_is_deterministic_per_row():
     assert (np.abs(cos - 1 / np.sqrt(1 + 128 * 0.01)) < 0.1).all()
 
 
+def test_oracle_generator_restatement_equals_the_library_generator(orc):
+    """The benchmark's CPU legs build their corpus with the oracle's restatement
+    of the generator; it must give the library's rows bit for bit (doc rows at
+    any offset, queries and their planted source docs)."""
+    for seed, n, dim, first in ((0x0DD5EED4, 300, 768, 0), (0x0DD5EED4, 200, 768, 9_999_800), (7, 65, 256, 12)):
+        a = ob.synth_docs(seed, n, dim, first=first)
+        b = orc.synth_docs(seed, n, dim, first=first)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+        qa, pa = ob.synth_queries(seed + 1, 10_000_000, 33, dim)
+        qb, pb = orc.synth_queries(seed + 1, 10_000_000, 33, dim)
+        assert np.array_equal(qa.view(np.uint32), qb.view(np.uint32)) and np.array_equal(pa, pb)
+
+
 def test_device_entry_points_fail_cleanly_without_a_gpu():
     try:
         import torch
@@ -207,3 +220,6 @@ def test_rank_and_selftest_entry_points_fail_cleanly_without_a_gpu():
     assert L.ovb_selftest_bounded_wait(None, None) == 1
     assert L.ovb_selftest_bounded_wait(C.byref(t), C.byref(w)) == 11
     assert L.ovb_index_search_device(None, 0, None, 0, 1, None, None, None) == 1
+    # the allocation-free entry point checks for a device before anything else
+    assert L.ovb_rankquant_search_noalloc(None, None, 0, 1, None, None, None) == 11
+    assert "CUDA" in L.ordvec_last_error().decode()

@@ -294,3 +294,57 @@ def test_rankquant_symmetric_scores_are_exact_centre_products(orc):
         assert np.array_equal(s[0], want[i[0]]), bits
         order = sorted(range(n), key=lambda d: (-want[d], d))
         assert i[0].tolist() == order, bits
+
+
+def test_rank_transform_is_a_stable_argsort_with_signed_zero_ties(orc):
+    """src/rank.rs:38-53 with cmp_finite_f32_then_index (src/util.rs:19-30):
+    equal values (-0.0 == +0.0 included) take ranks in index order.  numpy's
+    stable argsort orders -0.0 and +0.0 as equal too."""
+    rng = np.random.default_rng(11)
+    for d in (2, 8, 64, 768, 1024, 4096):
+        for trial in range(12):
+            v = rng.standard_normal(d).astype(np.float32)
+            if trial % 3 == 0:
+                v = np.round(v * 2) / 2  # heavy ties
+            if trial % 4 == 0:
+                v[::5] = -0.0
+                v[1::7] = 0.0
+            order = np.argsort(v, kind="stable")
+            want = np.empty(d, np.uint16)
+            want[order] = np.arange(d)
+            assert np.array_equal(orc.rank_transform(v), want), (d, trial)
+
+
+def test_one_pass_encoder_equals_the_separate_encoders(orc):
+    docs = orc.synth_docs(5, 700, 768)
+    words = np.empty(700 * 12, np.uint64)
+    packed = np.empty(700 * 192, np.uint8)
+    orc.encode_bitmap_rankquant(docs, 768, 192, 2, words, packed)
+    assert np.array_equal(words, orc.bitmap_encode(docs, 768, 192))
+    assert np.array_equal(packed, orc.rankquant_encode(docs, 768, 2))
+    p4 = np.empty(700 * 384, np.uint8)
+    orc.encode_bitmap_rankquant(docs, 768, 100, 4, None, p4)
+    assert np.array_equal(p4, orc.rankquant_encode(docs, 768, 4))
+
+
+def test_cpu_bitmap_two_stage_equals_the_scalar_oracle(orc):
+    """The timed CPU restatement (groups of 8 queries on the AVX-512 batched
+    scan, then the AVX-512 rerank) against the scalar checker: candidate rows
+    bit-exact in (overlap desc, id asc) order, including a final group of 3
+    queries; reranked ids equal to the FP64 ordering except within the float
+    tolerance."""
+    n, dim, n_top, nq, m, k = 9000, 768, 192, 19, 400, 20
+    docs = orc.synth_docs(9, n, dim)
+    qs, _ = orc.synth_queries(9, n, nq, dim)
+    words = orc.bitmap_encode(docs, dim, n_top)
+    packed = orc.rankquant_encode(docs, dim, 2)
+    s, i, cands = orc.cpu_bitmap_two_stage(words, packed, n, dim, n_top, 2, qs, m, k, 4, want_candidates=True)
+    for qi in range(nq):
+        want = orc.bitmap_top_m(words, n, dim, n_top, qs[qi], m)
+        assert np.array_equal(cands[qi], want), qi
+        s64 = orc.rq_scores_f64_subset(packed, dim, 2, qs[qi], want)
+        order = np.lexsort((want, -s64))[:k]
+        got64 = orc.rq_scores_f64_subset(packed, dim, 2, qs[qi], i[qi].astype(np.uint32))
+        tol = 1e-5 * np.maximum(np.abs(s64[order]), 1e-3)
+        assert np.all(np.abs(np.sort(got64)[::-1] - s64[order]) <= tol), qi
+        np.testing.assert_allclose(s[qi], got64, rtol=1e-5, atol=1e-6)
