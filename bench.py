@@ -178,6 +178,55 @@ def topk_agreement(orc, packed, dim, bits, queries, ids_a, ids_b):
     return False, ok, rows
 
 
+def split_error_stats(orc, packed, dim, bits, queries, ids, scores):
+    """Largest |score - FP64 score| and relative error (|d| / max(|s64|, 1e-3))
+    of returned (ids, scores) rows against the oracle's FP64 scores."""
+    max_abs = max_rel = 0.0
+    for qi in range(ids.shape[0]):
+        v = ids[qi] >= 0
+        s64 = orc.rq_scores_f64_subset(packed, dim, bits, queries[qi], ids[qi][v].astype(np.uint32))
+        d = np.abs(scores[qi][v].astype(np.float64) - s64)
+        if d.size:
+            max_abs = max(max_abs, float(d.max()))
+            max_rel = max(max_rel, float((d / np.maximum(np.abs(s64), 1e-3)).max()))
+    return max_abs, max_rel
+
+
+def rerank_report(ob, orc, torch, dev, rq, s1, d_q, queries, m, k, packed, sample, profile_fp64):
+    """The rerank of a two-stage batch: the default (split-BF16 on tcgen05 +
+    FP64 rescoring of the top 2k + 32) against the FP64-table rerank -- stage
+    times of both, and the error against the oracle's FP64 scores of the raw
+    split-BF16 scores and of the returned scores, over `sample` queries."""
+    nq = d_q.shape[0]
+    sp = torch.cuda.current_stream(dev).cuda_stream
+    d_s = torch.empty(nq * k, dtype=torch.float32, device=dev)
+    d_i = torch.empty(nq * k, dtype=torch.int64, device=dev)
+    out = {"form": "split-BF16 tcgen05 (codes exact in BF16, query hi+lo BF16, f32 accumulation) + margin test + "
+                   "FP64 rescoring of the top 2k+32"}
+    os.environ["OVB_RERANK_TC"] = "0"
+    try:
+        st = profile_fp64()
+    finally:
+        del os.environ["OVB_RERANK_TC"]
+    out["fp64_rerank_ms"], out["fp64_final_select_ms"] = st[4], st[5]
+    if orc is None or packed is None:
+        return out
+    ob.two_stage_search_device(rq, s1, d_q.data_ptr(), nq, m, k, d_s.data_ptr(), d_i.data_ptr(), sp,
+                               rerank="split_raw")
+    torch.cuda.synchronize(dev)
+    raw_s, raw_i = d_s.view(nq, k).cpu().numpy()[:sample], d_i.view(nq, k).cpu().numpy()[:sample]
+    ob.two_stage_search_device(rq, s1, d_q.data_ptr(), nq, m, k, d_s.data_ptr(), d_i.data_ptr(), sp)
+    torch.cuda.synchronize(dev)
+    ex_s, ex_i = d_s.view(nq, k).cpu().numpy()[:sample], d_i.view(nq, k).cpu().numpy()[:sample]
+    dim, bits = rq.dim, rq.bits
+    a, r = split_error_stats(orc, packed, dim, bits, queries[:sample], raw_i, raw_s)
+    out["split_bf16_max_abs_err_vs_fp64"], out["split_bf16_max_rel_err_vs_fp64"] = a, r
+    a, r = split_error_stats(orc, packed, dim, bits, queries[:sample], ex_i, ex_s)
+    out["rerank_max_abs_err_vs_fp64"], out["rerank_max_rel_err_vs_fp64"] = a, r
+    out["error_sample_queries"] = sample
+    return out
+
+
 def cpu_sample_size(probe_qps: float, budget_s: float, group: int, cap: int) -> int:
     q = int(probe_qps * budget_s) // group * group
     return max(group, min(cap, q))
@@ -466,6 +515,11 @@ def fastscan_run(ob, torch, dev, args, cpu: bool):
                              "sample": f"first {sample} of the {FS_NQ} queries, all host threads",
                              "identical_top10_vs_cpu": same, "equal_up_to_fp64_near_ties": tol_same,
                              "rows_differing": rows}
+        out["rerank"] = rerank_report(
+            ob, orc, torch, dev, rq, fs, d_q, queries, FS_M, FS_K, packed, 128,
+            lambda: ob.two_stage_profile(rq, fs, d_q.data_ptr(), FS_NQ, FS_M, FS_K, d_s.data_ptr(), d_i.data_ptr(),
+                                         sp))
+        out["rerank"]["split_rerank_ms"], out["rerank"]["split_final_select_ms"] = st[4], st[5]
     return out
 
 
@@ -1018,6 +1072,10 @@ def main():
         "build_s": build_s,
         "clocks": clock_info,
     }
+    line["rerank"] = rerank_report(
+        ob, orc, torch, dev, rq, bm, d_q, queries, M, K, h_packed, 128,
+        lambda: ob.two_stage_profile(rq, bm, d_q.data_ptr(), NQ, M, K, d_s.data_ptr(), d_i.data_ptr(), sp))
+    line["rerank"]["split_rerank_ms"], line["rerank"]["split_final_select_ms"] = stages[4], stages[5]
     if cpu:
         line["codes_identical_to_oracle"] = bool(np.array_equal(bm.payload().view(np.uint64), h_words)
                                                  and np.array_equal(rq.payload(), h_packed))

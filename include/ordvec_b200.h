@@ -293,6 +293,30 @@ ordvec_status_t ovb_two_stage_search_device(const ordvec_index_t *rq,
                                             const float *d_queries, uint64_t nq, uint64_t m,
                                             uint64_t k, float *d_scores, int64_t *d_ids,
                                             void *stream);
+/* How the two-stage pipelines rerank (no counterpart in the reference, whose
+ * rerank is its asymmetric subset scorer, src/quant.rs:1126-1281):
+ *   OVB_RERANK_AUTO       the split-BF16 tensor-core rerank where the shape
+ *                         allows it (dim % 64 == 0, 16 <= dim*bits/8 <= 256 and a
+ *                         multiple of 16, >= 16 queries, m >= 4k + 64), else FP64
+ *   OVB_RERANK_FP64       every candidate scored in FP64 (per-query tables)
+ *   OVB_RERANK_SPLIT      split-BF16 scores (codes exact in BF16, query = hi + lo
+ *                         BF16, f32 accumulation on tcgen05), then the top
+ *                         2k + 32 by that score rescored in FP64 after a margin
+ *                         test against the stated error bound: the same ids as
+ *                         FP64 (a failed margin test reranks the batch in FP64)
+ *   OVB_RERANK_SPLIT_RAW  the split-BF16 scores themselves, top-k by them (for
+ *                         measuring the split's error against FP64)
+ * The default calls (ovb_two_stage_search, _device, _profile) use AUTO. */
+#define OVB_RERANK_AUTO 0u
+#define OVB_RERANK_FP64 1u
+#define OVB_RERANK_SPLIT 2u
+#define OVB_RERANK_SPLIT_RAW 3u
+/* ovb_two_stage_search_device with an explicit OVB_RERANK_* mode. */
+ordvec_status_t ovb_two_stage_search_device_ex(const ordvec_index_t *rq,
+                                               const ordvec_index_t *stage1,
+                                               const float *d_queries, uint64_t nq, uint64_t m,
+                                               uint64_t k, float *d_scores, int64_t *d_ids,
+                                               void *stream, uint32_t rerank_mode);
 /* Same as ovb_two_stage_search_device, synchronous, with CUDA events recorded
  * on `stream` between the pipeline stages; stage_ms[0..5] receives the device
  * time of: query prep, stage-1 candidate threshold (sample scan + select; 0

@@ -111,6 +111,7 @@ SIGNATURES = {
     "ovb_multibucket_top_m": (S, [P, P, U64, P, U64, P]),
     "ovb_two_stage_search": (S, [P, P, P, U64, U64, U64, P, P]),
     "ovb_two_stage_search_device": (S, [P, P, P, U64, U64, U64, P, P, P]),
+    "ovb_two_stage_search_device_ex": (S, [P, P, P, U64, U64, U64, P, P, P, U32]),
     "ovb_two_stage_profile": (S, [P, P, P, U64, U64, U64, P, P, P, P]),
     "ovb_rankquant_search_noalloc": (S, [P, P, U64, U64, P, P, P]),
     "ovb_last_launch_count": (U64, []),

@@ -862,6 +862,28 @@ ordvec_status_t ovb_two_stage_search_device(const ordvec_index_t* rq, const ordv
   });
 }
 
+ordvec_status_t ovb_two_stage_search_device_ex(const ordvec_index_t* rq, const ordvec_index_t* stage1,
+                                               const float* d_queries, uint64_t nq, uint64_t m, uint64_t k,
+                                               float* d_scores, int64_t* d_ids, void* stream, uint32_t rerank_mode) {
+  return boundary([&] {
+    if (rerank_mode > OVB_RERANK_SPLIT_RAW) fail(ORDVEC_STATUS_BAD_ARGUMENT, "unknown rerank mode");
+    const Index& r = as_index(rq);
+    const Index& s = as_index(stage1);
+    need_queries(d_queries, nq);
+    if (!nq || !k || !r.n) return;
+    if (!d_scores || !d_ids) fail(ORDVEC_STATUS_NULL_POINTER, "output pointer is NULL");
+    Workspace& w = workspace();
+    cudaStream_t st = (cudaStream_t)stream;
+    struct Mode {
+      Workspace& w;
+      Mode(Workspace& ws, uint32_t m_) : w(ws) { w.rerank_mode = m_; }
+      ~Mode() { w.rerank_mode = OVB_RERANK_AUTO; }
+    } guard(w, rerank_mode);
+    uint32_t got = engine_two_stage(r, s, d_queries, nq, m, k, w, st);
+    launch_keys_to_results(w.out_keys.as<uint32_t>(), w.out_ids.as<uint32_t>(), nq * got, 0, 0, d_scores, d_ids, st);
+  });
+}
+
 ordvec_status_t ovb_selftest_bounded_wait(uint32_t* timed_out, uint64_t* waited_ns) {
   return boundary([&] {
     if (!timed_out || !waited_ns) fail(ORDVEC_STATUS_NULL_POINTER, "output pointer is NULL");

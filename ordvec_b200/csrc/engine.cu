@@ -662,6 +662,68 @@ uint32_t engine_fastscan_full(const Index& fs, const float* d_q, uint64_t nq, ui
   return ke;
 }
 
+// How a two-stage search reranks its uniform candidate rows (me per query,
+// top-ke): the caller's OVB_RERANK_* mode, or for OVB_RERANK_AUTO the
+// split-BF16 tensor-core rerank when the index shape allows it, the batch has
+// at least 16 queries and the rows are long enough for the exact form's
+// rescoring set (kp below) to be a real subset; OVB_RERANK_TC=0/1 overrides
+// the automatic choice.
+static uint32_t rerank_mode(const Workspace& w, const Index& rq, uint64_t nq, uint32_t me, uint32_t ke) {
+  if (w.rerank_mode == OVB_RERANK_SPLIT_RAW) return rerank_tc_eligible(rq.dim, rq.bits) ? w.rerank_mode : OVB_RERANK_FP64;
+  if (w.rerank_mode != OVB_RERANK_AUTO) return w.rerank_mode;
+  if (!rerank_tc_eligible(rq.dim, rq.bits)) return OVB_RERANK_FP64;
+  const char* e = getenv("OVB_RERANK_TC");
+  if (e && e[0] == '0') return OVB_RERANK_FP64;
+  if (e && e[0] == '1') return OVB_RERANK_SPLIT;
+  return nq >= 16 && (uint64_t)me >= 4ull * ke + 64 ? OVB_RERANK_SPLIT : OVB_RERANK_FP64;
+}
+
+// Split-BF16 rerank of the uniform candidate rows in w.sel_ids (me per query):
+// split queries, the tensor-core rerank (keys2), then either the raw top-ke of
+// the split scores (raw) or the exact form -- the top-kp by split score with
+// kp = min(me, 2 ke + 32), the margin test (the kp-th split score more than
+// twice the error bound below the k-th, so every candidate that can reach the
+// exact top-ke is among the kp), FP64 rescoring of the kp and the top-ke of
+// those.  A query that fails the margin test makes the exact form return
+// false after one synchronisation; the caller then reranks the batch in FP64.
+static bool split_rerank(const Index& rq, const float* qu, uint64_t nq, uint32_t me, uint32_t ke, float inv_norm,
+                         bool raw, Workspace& w, cudaStream_t st) {
+  if (!rerank_tc_eligible(rq.dim, rq.bits)) return false;
+  const uint32_t dim = rq.dim, bits = rq.bits, id_bits = bits_for(rq.n - 1);
+  const uint8_t* codes = rq.codes.as<uint8_t>();
+  const uint32_t* cand = w.sel_ids.as<uint32_t>();
+  void* qs = w.q_split.ensure(nq * dim * 4);
+  float* l1 = (float*)w.q_l1.ensure(nq * 4);
+  launch_split_queries(qu, nq, dim, qs, l1, st);
+  uint32_t* keys = (uint32_t*)w.keys2.ensure(nq * me * 4);
+  launch_rerank_tc(codes, rq.n, dim, bits, qs, nq, cand, me, me, inv_norm, keys, w.tc_err_word(st), st);
+  w.mark(st, 4);
+  uint32_t* ok = w.out_keys.as<uint32_t>();
+  uint32_t* oi = w.out_ids.as<uint32_t>();
+  if (raw) {
+    select_rows(w, keys, cand, nullptr, me, me, nq, ke, 32, id_bits, ok, oi, st);
+    w.mark(st, 5);
+    return true;
+  }
+  const uint32_t kp = std::min<uint32_t>(me, 2 * ke + 32);
+  uint32_t* ck = (uint32_t*)w.rr_keys.ensure(nq * kp * 4);
+  uint32_t* ci = (uint32_t*)w.rr_ids.ensure(nq * kp * 4);
+  uint32_t* flag = (uint32_t*)w.rr_flag.ensure(4);
+  uint32_t* flag_h = (uint32_t*)w.rr_flag_host.ensure(4);
+  select_rows(w, keys, cand, nullptr, me, me, nq, kp, 32, id_bits, ck, ci, st);
+  OVB_CUDA(cudaMemsetAsync(flag, 0, 4, st));
+  launch_split_margin(ck, nq, kp, ke, l1, split_error_bound(dim, bits, inv_norm), flag, st);
+  uint64_t* off = (uint64_t*)w.off.ensure((nq + 1) * 8);
+  launch_uniform_offsets(off, nq, kp, st);
+  uint32_t* k2 = (uint32_t*)w.rr_keys2.ensure(nq * kp * 4);
+  launch_asym_subset(codes, dim, bits, qu, nq, off, ci, kp, inv_norm, k2, st);
+  select_rows(w, k2, ci, nullptr, kp, kp, nq, ke, 32, id_bits, ok, oi, st);
+  w.mark(st, 5);
+  OVB_CUDA(cudaMemcpyAsync(flag_h, flag, 4, cudaMemcpyDeviceToHost, st));
+  OVB_CUDA(cudaStreamSynchronize(st));
+  return *flag_h == 0;
+}
+
 uint32_t engine_two_stage(const Index& rq, const Index& s1, const float* d_q, uint64_t nq,
                           uint64_t m, uint64_t k, Workspace& w, cudaStream_t st) {
   require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "two-stage rerank");
@@ -684,17 +746,21 @@ uint32_t engine_two_stage(const Index& rq, const Index& s1, const float* d_q, ui
   }
   const uint32_t ke = (uint32_t)(k < me ? k : me);
   if (!ke) return ke;
-  uint64_t* off = (uint64_t*)w.off.ensure((nq + 1) * 8);
-  launch_uniform_offsets(off, nq, me, st);
   const float inv_norm = inv_rankquant_norm(rq.dim, rq.bits);
-  uint32_t* keys = (uint32_t*)w.keys2.ensure(nq * me * 4);
-  launch_asym_subset(rq.codes.as<uint8_t>(), rq.dim, rq.bits, qu, nq, off, w.sel_ids.as<uint32_t>(), me,
-                     inv_norm, keys, st);
-  w.mark(st, 4);
   uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
   uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
+  const uint32_t id_bits = bits_for(rq.n - 1);
+  const uint32_t* cand = w.sel_ids.as<uint32_t>();
+  const uint32_t mode = rerank_mode(w, rq, nq, me, ke);
+  if (mode != OVB_RERANK_FP64 && split_rerank(rq, qu, nq, me, ke, inv_norm, mode == OVB_RERANK_SPLIT_RAW, w, st))
+    return ke;
+  uint64_t* off = (uint64_t*)w.off.ensure((nq + 1) * 8);
+  launch_uniform_offsets(off, nq, me, st);
+  uint32_t* keys = (uint32_t*)w.keys2.ensure(nq * me * 4);
+  launch_asym_subset(rq.codes.as<uint8_t>(), rq.dim, rq.bits, qu, nq, off, cand, me, inv_norm, keys, st);
+  w.mark(st, 4);
   // rows are uniform (me candidates each): the strided form, not offsets
-  select_rows(w, keys, w.sel_ids.as<uint32_t>(), nullptr, me, me, nq, ke, 32, bits_for(rq.n - 1), ok, oi, st);
+  select_rows(w, keys, cand, nullptr, me, me, nq, ke, 32, id_bits, ok, oi, st);
   w.mark(st, 5);
   return ke;
 }

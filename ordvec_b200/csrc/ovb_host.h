@@ -102,6 +102,11 @@ struct Workspace {
   DevBuf smp_keys, thr_keys, thr_ids, f_keys, f_ids, f_cnt, f_flag;
   // split-BF16 rank scan: [hi; lo] query rows and |q|_1
   DevBuf q_split, q_l1;
+  // split-BF16 rerank: top-kp split keys / ids per query, their FP64 keys, the margin flag
+  DevBuf rr_keys, rr_ids, rr_keys2, rr_flag;
+  HostBuf rr_flag_host;
+  // how engine_two_stage reranks (OVB_RERANK_* of ordvec_b200.h; 0 = auto)
+  uint32_t rerank_mode = 0;
   uint64_t split_kp = 0;  // largest candidate count the last exact split search settled on
   bool cand_unordered = false;  // set while a two-stage search selects its stage-1 set
   HostBuf pinned, f_flag_host;

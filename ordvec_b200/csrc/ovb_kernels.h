@@ -132,6 +132,14 @@ void launch_rank_filter_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint3
 void launch_split_margin(const uint32_t* sel_keys, uint64_t nq, uint32_t kp, uint32_t k, const float* l1,
                          float bound_per_l1, uint32_t* flag, cudaStream_t stream);
 
+// ---- K5-TC split-BF16 candidate rerank on tcgen05 (rerank_tc.cu) ---------------
+// dim % 64 == 0 and 16 <= dim * bits / 8 <= 256, a multiple of 16
+bool rerank_tc_eligible(uint32_t dim, uint32_t bits);
+// keys[q * ld + j] = desc key of the split-BF16 score of candidate cands[q * ld + j], j < m
+void launch_rerank_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_t bits, const void* q_split,
+                      uint64_t nq, const uint32_t* cands, uint64_t ld, uint32_t m, float inv_norm, uint32_t* keys,
+                      uint32_t* err, cudaStream_t stream);
+
 // ---- self-test (selftest.cu): out[0] = 1 when a bounded mbarrier wait on a
 // barrier nothing arrives at gave up, out[1..2] = the nanoseconds it waited
 void launch_wait_probe(uint32_t* d_out, cudaStream_t stream);
