@@ -656,6 +656,8 @@ def profile_case(case: str):
       multibucket MultiBucketBitmap(768, 2) N=2M: diagonal-weight top-2000 of 1
                 query per call (multibucket_rows_kernel), 3 calls
       encode    RankQuant(768, 2).add of 1M docs, twice (rank_encode_kernel)
+      rerank    Bitmap(768, 192) top-2000 -> RankQuant b=2 top-100 of 1024 queries,
+                N=2M, twice (rerank_tc_kernel, asym_table_kernel rescoring)
     Each search runs more than once so captures can skip the first call."""
     import ordvec_b200 as ob
 
@@ -675,6 +677,16 @@ def profile_case(case: str):
         q, _ = ob.synth_queries(0x0DD5EED5, n, 4, 768)
         for i in range(3):
             mb.top_m_bilinear_batched(q[i:i + 1], mb.diagonal_weights(), 2000)
+    elif case == "rerank":
+        n = 2_000_000
+        rq, bm = ob.RankQuant(768, 2), ob.Bitmap(768, 192)
+        for first in range(0, n, 1_000_000):
+            d = ob.synth_docs(0x0DD5EED4, 1_000_000, 768, first=first)
+            rq.add(d)
+            bm.add(d)
+        q, _ = ob.synth_queries(0x0DD5EED5, n, 1024, 768)
+        for _ in range(2):
+            ob.two_stage_search(rq, bm, q, 2000, 100)
     elif case == "encode":
         rq = ob.RankQuant(768, 2)
         d = ob.synth_docs(0x0DD5EED4, 1_000_000, 768)
@@ -904,7 +916,7 @@ def main():
                     help="the extra configurations (auto: on a single GPU only)")
     ap.add_argument("--profile-case",
                     choices=["bitmap", "bitmap10m", "popc", "rank", "fastscan", "plain", "rankfull", "multibucket",
-                             "encode"],
+                             "encode", "rerank"],
                     help="run one small kernel workload for an ncu capture and exit")
     args = ap.parse_args()
     if args.profile_case:

@@ -765,4 +765,39 @@ uint32_t engine_two_stage(const Index& rq, const Index& s1, const float* d_q, ui
   return ke;
 }
 
+uint32_t engine_two_stage_ragged(const Index& rq, const Index& s1, const float* d_q, uint64_t nq,
+                                 const uint64_t* m_of, uint64_t k, Workspace& w, cudaStream_t st) {
+  require_kind(rq, ORDVEC_INDEX_KIND_RANK_QUANT, "two-stage rerank");
+  if (s1.dim != rq.dim) fail(ORDVEC_STATUS_DIM_MISMATCH, "stage-1 index dim must match RankQuant dim");
+  if (s1.n != rq.n) fail(ORDVEC_STATUS_BAD_ARGUMENT, "stage-1 index len must match RankQuant len");
+  w.mark(st, 0);
+  if (!nq || !k) return 0;
+  uint64_t m_max = 0;
+  for (uint64_t q = 0; q < nq; q++) m_max = std::max(m_max, m_of[q]);
+  if (!m_max) return 0;
+  const float* qu = normalised(w, d_q, nq, rq.dim, st);
+  // ordered rows: each query's own top-m is the prefix of its top-m_max
+  const uint32_t me = engine_candidates(s1, d_q, nq, m_max, nullptr, w, st, qu);
+  const uint32_t ke = (uint32_t)(k < me ? k : me);
+  if (!ke) return ke;
+  uint64_t* h_off = (uint64_t*)w.off_host.ensure((nq + 1) * 8);
+  OVB_CUDA(cudaStreamSynchronize(st));  // the pinned offsets may still feed an earlier copy
+  h_off[0] = 0;
+  for (uint64_t q = 0; q < nq; q++) h_off[q + 1] = h_off[q] + std::min<uint64_t>(m_of[q], me);
+  uint64_t* off = (uint64_t*)w.off.ensure((nq + 1) * 8);
+  OVB_CUDA(cudaMemcpyAsync(off, h_off, (nq + 1) * 8, cudaMemcpyHostToDevice, st));
+  const uint64_t total = h_off[nq];
+  uint32_t* cand = (uint32_t*)w.csr_ids.ensure(total * 4 + 4);
+  launch_prefix_compact(w.sel_ids.as<uint32_t>(), me, off, nq, cand, st);
+  uint32_t* keys = (uint32_t*)w.keys2.ensure(total * 4 + 4);
+  launch_asym_subset(rq.codes.as<uint8_t>(), rq.dim, rq.bits, qu, nq, off, cand, me, inv_rankquant_norm(rq.dim, rq.bits),
+                     keys, st);
+  w.mark(st, 4);
+  uint32_t* ok = (uint32_t*)w.out_keys.ensure(nq * ke * 4);
+  uint32_t* oi = (uint32_t*)w.out_ids.ensure(nq * ke * 4);
+  select_rows(w, keys, cand, off, 0, 0, nq, ke, 32, bits_for(rq.n - 1), ok, oi, st);
+  w.mark(st, 5);
+  return ke;
+}
+
 }  // namespace ovb

@@ -121,9 +121,13 @@ void capture(Plan& p) {
   OVB_CUDA(cudaGraphInstantiate(&p.exec, p.graph, 0));
 }
 
-// Runs one group through its plan: queries (host, nq x dim) -> scores / ids
-// (host, nq x ke).  The first call sizes, tunes and captures.
-void run_plan(Plan& p, const float* h_q, float* h_s, int64_t* h_i) {
+// Runs one group through its plan in two phases, so the groups of a mixed
+// batch overlap on the device: plan_enqueue copies the queries in and, once a
+// graph exists, replays it and queues the copies of the margin flag and the
+// results (host in, host out, nothing waited for); plan_finish waits for the
+// plan's stream and, on the first call or when the flag shows kp was too small
+// for some query, runs the exact pipeline and (re)captures the graph.
+bool plan_enqueue(Plan& p, const float* h_q, float* h_s, int64_t* h_i) {
   Workspace& w = *p.w;
   cudaStream_t st = w.stream;
   const Index& ix = *p.ix;
@@ -133,32 +137,46 @@ void run_plan(Plan& p, const float* h_q, float* h_s, int64_t* h_i) {
   int64_t* di = (int64_t*)p.di.ensure(p.nq * ke * 8);
   uint32_t* hflag = (uint32_t*)p.hflag.ensure(4);
   OVB_CUDA(cudaMemcpyAsync(dq, h_q, p.nq * ix.dim * 4, cudaMemcpyHostToDevice, st));
+  if (!p.exec) return false;
+  OVB_CUDA(cudaGraphLaunch(p.exec, st));
+  OVB_CUDA(cudaMemcpyAsync(hflag, p.dflag.p, 4, cudaMemcpyDeviceToHost, st));
+  OVB_CUDA(cudaMemcpyAsync(h_s, ds, p.nq * ke * 4, cudaMemcpyDeviceToHost, st));
+  OVB_CUDA(cudaMemcpyAsync(h_i, di, p.nq * ke * 8, cudaMemcpyDeviceToHost, st));
+  return true;
+}
+
+void plan_finish(Plan& p, bool enqueued, float* h_s, int64_t* h_i) {
+  Workspace& w = *p.w;
+  cudaStream_t st = w.stream;
+  const Index& ix = *p.ix;
+  const uint32_t ke = (uint32_t)std::min<uint64_t>(p.k, ix.n);
+  OVB_CUDA(cudaStreamSynchronize(st));
   bool done = false;
-  if (p.exec) {
-    OVB_CUDA(cudaGraphLaunch(p.exec, st));
-    OVB_CUDA(cudaMemcpyAsync(hflag, p.dflag.p, 4, cudaMemcpyDeviceToHost, st));
-    OVB_CUDA(cudaStreamSynchronize(st));
+  if (enqueued) {
     check_tc_errors(w);
     p.replays++;
-    done = *hflag == 0;
+    done = *(uint32_t*)p.hflag.p == 0;
   }
-  if (!done) {  // first call, or kp was too small for some query: the exact pipeline
-    engine_rankquant_full_split(ix, dq, p.nq, p.k, true, w, st, p.qpt);
-    launch_keys_to_results(w.out_keys.as<uint32_t>(), w.out_ids.as<uint32_t>(), p.nq * ke, 0, 0, ds, di, st);
-    OVB_CUDA(cudaStreamSynchronize(st));
-    check_tc_errors(w);
-    const uint64_t kp = std::max<uint64_t>(w.split_kp, ke);
-    if (!p.no_graph && (!p.exec || kp > p.kp)) {
+  if (done) return;
+  // first call, or kp was too small for some query: the exact pipeline
+  float* dq = p.dq.as<float>();
+  float* ds = p.ds.as<float>();
+  int64_t* di = p.di.as<int64_t>();
+  engine_rankquant_full_split(ix, dq, p.nq, p.k, true, w, st, p.qpt);
+  launch_keys_to_results(w.out_keys.as<uint32_t>(), w.out_ids.as<uint32_t>(), p.nq * ke, 0, 0, ds, di, st);
+  OVB_CUDA(cudaStreamSynchronize(st));
+  check_tc_errors(w);
+  const uint64_t kp = std::max<uint64_t>(w.split_kp, ke);
+  if (!p.no_graph && (!p.exec || kp > p.kp)) {
+    p.drop_graph();
+    p.kp = kp;
+    if (!p.qpt) p.qpt = autotune_tile(p);
+    try {
+      capture(p);
+    } catch (const CudaError&) {
       p.drop_graph();
-      p.kp = kp;
-      if (!p.qpt) p.qpt = autotune_tile(p);
-      try {
-        capture(p);
-      } catch (const CudaError&) {
-        p.drop_graph();
-        p.no_graph = true;
-        cudaGetLastError();
-      }
+      p.no_graph = true;
+      cudaGetLastError();
     }
   }
   OVB_CUDA(cudaMemcpyAsync(h_s, ds, p.nq * ke * 4, cudaMemcpyDeviceToHost, st));
@@ -205,16 +223,15 @@ bool mixed_plan_info(const Index& ix, uint64_t nq, uint64_t k, uint32_t* qpt, ui
   return true;
 }
 
-// One group: nq queries of one index with k; host in, host out (nq x ke).
-uint32_t mixed_group(const Index& ix, const float* h_q, uint64_t nq, uint64_t k, float* h_s, int64_t* h_i) {
+// Whether a group of nq queries of index ix with top-k runs through a plan.
+bool group_uses_plan(const Index& ix, uint64_t nq, uint64_t k) {
+  return graphs_enabled() && rank_tc_eligible(ix.dim, ix.bits) && split_fixed_fits(ix, nq, k);
+}
+
+// One group without a plan: nq queries of one index with k; host in, host out (nq x ke).
+uint32_t mixed_group_direct(const Index& ix, const float* h_q, uint64_t nq, uint64_t k, float* h_s, int64_t* h_i) {
   const uint32_t ke = (uint32_t)std::min<uint64_t>(k, ix.n);
   if (!ke || !nq) return ke;
-  if (graphs_enabled() && rank_tc_eligible(ix.dim, ix.bits) && split_fixed_fits(ix, nq, k)) {
-    Plan& p = plan_for(ix, nq, ke);
-    std::lock_guard<std::mutex> lk(p.mu);
-    run_plan(p, h_q, h_s, h_i);
-    return ke;
-  }
   Workspace& w = workspace();
   float* dq = (float*)w.q_raw.ensure(nq * ix.dim * 4);
   OVB_CUDA(cudaMemcpyAsync(dq, h_q, nq * ix.dim * 4, cudaMemcpyHostToDevice, w.stream));
@@ -262,19 +279,51 @@ ordvec_status_t ovb_rankquant_search_mixed(const ordvec_index_t* const* indices,
       scores[v] = -std::numeric_limits<float>::infinity();
       ids[v] = -1;
     }
-    thread_local HostBuf stage_q, stage_s, stage_i;  // pinned group staging
+    // pinned staging per group: the groups' copies and replays are in flight together
+    thread_local std::vector<std::unique_ptr<HostBuf>> sq, ss, si;
+    while (sq.size() < n_indices) {
+      sq.emplace_back(new HostBuf());
+      ss.emplace_back(new HostBuf());
+      si.emplace_back(new HostBuf());
+    }
+    auto stage_q = [&](uint32_t j) -> HostBuf& { return *sq[j]; };
+    auto stage_s = [&](uint32_t j) -> HostBuf& { return *ss[j]; };
+    auto stage_i = [&](uint32_t j) -> HostBuf& { return *si[j]; };
+    std::vector<uint64_t> kg(n_indices, 0), keg(n_indices, 0);
+    std::vector<Plan*> plan(n_indices, nullptr);
+    std::vector<std::unique_lock<std::mutex>> locks;
+    std::vector<char> enqueued(n_indices, 0);
+    // phase 1: stage every group; groups with a plan replay its graph (no wait)
     for (uint32_t j = 0; j < n_indices; j++) {
       const auto& g = groups[j];
       if (g.empty()) continue;
-      uint64_t kg = 0;
-      for (uint64_t i : g) kg = std::max<uint64_t>(kg, k_of_query[i]);
+      for (uint64_t i : g) kg[j] = std::max<uint64_t>(kg[j], k_of_query[i]);
       const uint64_t nqg = g.size();
-      const uint64_t ke = std::min<uint64_t>(kg, ix[j]->n);
-      float* hq = (float*)stage_q.ensure(nqg * dim * 4);
-      float* hs = (float*)stage_s.ensure(std::max<uint64_t>(nqg * ke, 1) * 4);
-      int64_t* hi = (int64_t*)stage_i.ensure(std::max<uint64_t>(nqg * ke, 1) * 8);
+      keg[j] = std::min<uint64_t>(kg[j], ix[j]->n);
+      float* hq = (float*)stage_q(j).ensure(nqg * dim * 4);
+      stage_s(j).ensure(std::max<uint64_t>(nqg * keg[j], 1) * 4);
+      stage_i(j).ensure(std::max<uint64_t>(nqg * keg[j], 1) * 8);
       for (uint64_t r = 0; r < nqg; r++) std::copy(queries + g[r] * dim, queries + (g[r] + 1) * dim, hq + r * dim);
-      const uint32_t got = mixed_group(*ix[j], hq, nqg, kg, hs, hi);
+      if (keg[j] && group_uses_plan(*ix[j], nqg, kg[j])) {
+        plan[j] = &plan_for(*ix[j], nqg, (uint32_t)keg[j]);
+        locks.emplace_back(plan[j]->mu);  // plans of one call are distinct; taken in group order
+        enqueued[j] = plan_enqueue(*plan[j], hq, (float*)stage_s(j).p, (int64_t*)stage_i(j).p);
+      }
+    }
+    // phase 2: finish every group and scatter its rows (each row keeps its own k)
+    for (uint32_t j = 0; j < n_indices; j++) {
+      const auto& g = groups[j];
+      if (g.empty() || !keg[j]) continue;
+      const uint64_t nqg = g.size();
+      float* hs = (float*)stage_s(j).p;
+      int64_t* hi = (int64_t*)stage_i(j).p;
+      uint64_t got;
+      if (plan[j]) {
+        plan_finish(*plan[j], enqueued[j] != 0, hs, hi);
+        got = keg[j];
+      } else {
+        got = mixed_group_direct(*ix[j], (const float*)stage_q(j).p, nqg, kg[j], hs, hi);
+      }
       for (uint64_t r = 0; r < nqg; r++) {
         const uint64_t i = g[r];
         const uint64_t keep = std::min<uint64_t>(k_of_query[i], got);

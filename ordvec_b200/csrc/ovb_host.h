@@ -107,6 +107,9 @@ struct Workspace {
   HostBuf rr_flag_host;
   // how engine_two_stage reranks (OVB_RERANK_* of ordvec_b200.h; 0 = auto)
   uint32_t rerank_mode = 0;
+  // per-query candidate counts of a ragged two-stage batch: CSR offsets and rows
+  HostBuf off_host;
+  DevBuf csr_ids;
   uint64_t split_kp = 0;  // largest candidate count the last exact split search settled on
   bool cand_unordered = false;  // set while a two-stage search selects its stage-1 set
   HostBuf pinned, f_flag_host;
@@ -170,6 +173,14 @@ uint32_t engine_fastscan_full(const Index& fs, const float* d_q, uint64_t nq, ui
                               Workspace& w, cudaStream_t st);
 uint32_t engine_two_stage(const Index& rq, const Index& s1, const float* d_q, uint64_t nq,
                           uint64_t m, uint64_t k, Workspace& w, cudaStream_t st);
+// Two-stage search with its own candidate count per query (m_of[q], each
+// already clamped to n): stage 1 selects the ordered top-max(m_of) of every
+// query, so query q's own top-m_of[q] is the prefix of its row; the prefixes
+// are reranked and each output row holds the top-min(k, m_of[q]) (stride
+// min(k, max(m_of)), sentinel padded) -- row q equals a search of query q
+// alone with m_of[q] candidates.
+uint32_t engine_two_stage_ragged(const Index& rq, const Index& s1, const float* d_q, uint64_t nq,
+                                 const uint64_t* m_of, uint64_t k, Workspace& w, cudaStream_t st);
 uint64_t default_candidate_count(uint64_t k, uint64_t space);
 uint64_t engine_keys_budget();  // bytes a key matrix chunk may take
 // engine_rankquant_split_fixed can run nq queries of top-k in one chunk

@@ -175,6 +175,10 @@ void launch_finite_flag(const float* x, uint64_t count, uint32_t* flag, cudaStre
 
 // helper: key32 -> float score / sentinel mapping and uniform offsets
 void launch_uniform_offsets(uint64_t* off, uint64_t nq, uint64_t m, cudaStream_t stream);
+// CSR rows from prefixes: row q of dst (at off[q]) = the first off[q+1] - off[q]
+// entries of row q of src (row stride ld)
+void launch_prefix_compact(const uint32_t* src, uint64_t ld, const uint64_t* off, uint64_t nq, uint32_t* dst,
+                           cudaStream_t stream);
 // ids[i] >= n (sentinels of underfull select rows) -> 0, so a gather stays in bounds
 void launch_clamp_ids(uint32_t* ids, uint64_t count, uint32_t n, cudaStream_t stream);
 void launch_keys_to_results(const uint32_t* keys, const uint32_t* ids, uint64_t count,

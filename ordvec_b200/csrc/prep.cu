@@ -271,6 +271,14 @@ void launch_finite_flag(const float* x, uint64_t count, uint32_t* flag, cudaStre
 }
 
 namespace {
+// Row q's first off[q+1] - off[q] entries of src (row stride ld) -> dst[off[q] ..]
+__global__ void prefix_compact_kernel(const uint32_t* __restrict__ src, uint64_t ld, const uint64_t* __restrict__ off,
+                                      uint32_t* __restrict__ dst) {
+  const uint64_t q = blockIdx.x;
+  const uint64_t a = off[q], len = off[q + 1] - a;
+  for (uint64_t j = threadIdx.x; j < len; j += blockDim.x) dst[a + j] = src[q * ld + j];
+}
+
 __global__ void clamp_ids_kernel(uint32_t* ids, uint64_t count, uint32_t n) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x)
     if (ids[i] >= n) ids[i] = 0;
@@ -282,6 +290,14 @@ void launch_clamp_ids(uint32_t* ids, uint64_t count, uint32_t n, cudaStream_t st
   uint64_t blocks = ceil_div(count, 256);
   if (blocks > 148 * 8) blocks = 148 * 8;
   clamp_ids_kernel<<<(unsigned)blocks, 256, 0, stream>>>(ids, count, n);
+  launched();
+}
+
+void launch_prefix_compact(const uint32_t* src, uint64_t ld, const uint64_t* off, uint64_t nq, uint32_t* dst,
+                           cudaStream_t stream) {
+  if (!nq) return;
+  if (nq > 0x7FFFFFFFull) throw std::invalid_argument("prefix compaction: too many rows");
+  prefix_compact_kernel<<<(unsigned)nq, 256, 0, stream>>>(src, ld, off, dst);
   launched();
 }
 

@@ -75,6 +75,7 @@ struct RtArgs {
   uint32_t bpv;  // bytes per packed row
   uint64_t nq;
   uint32_t nt;  // B rows per tile (2 per query)
+  uint32_t q_tiles;  // query tiles; CTA b covers query tile b % q_tiles of doc tile b / q_tiles
   uint32_t block_stride;  // logical 32-doc block ub reads physical block ub * block_stride
   float inv_norm;
   // dense output (keys != null): keys[q * ld + u], u = logical doc
@@ -125,7 +126,10 @@ __global__ void __launch_bounds__(kRtThreads, 1)
   RtSmem& S = *reinterpret_cast<RtSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const uint32_t nt = a.nt;
-  const uint64_t r0 = (uint64_t)blockIdx.y * nt;  // first B row of the tile
+  // query tiles vary fastest over the linear grid, so the CTAs of one doc tile
+  // run together and its codes cross HBM once (the others read them from L2)
+  const uint64_t dtile = blockIdx.x / a.q_tiles;
+  const uint64_t r0 = (uint64_t)(blockIdx.x % a.q_tiles) * nt;  // first B row of the tile
   const uint64_t qb = r0 / 2;                     // first query of the tile
   const uint32_t nqt = (uint32_t)((a.nq - qb) < nt / 2 ? (a.nq - qb) : nt / 2);
   const uint32_t n_kb = a.dim / 64;
@@ -215,7 +219,7 @@ __global__ void __launch_bounds__(kRtThreads, 1)
     {
       uint32_t t0, t1;
       nibble_table<BITS>((uint32_t)lane, t0, t1);
-      const uint64_t pb = ((uint64_t)blockIdx.x * 8 + (r >> 5)) * a.block_stride;
+      const uint64_t pb = (dtile * 8 + (r >> 5)) * a.block_stride;
       const uint64_t doc = pb * 32 + (r & 31);
       const bool valid = pb < n_blocks && doc < a.n;
       // this thread's 4 * BITS code bytes of each K-block (8 * BITS bytes per K-block row)
@@ -303,9 +307,9 @@ __global__ void __launch_bounds__(kRtThreads, 1)
       const uint32_t eg = (uint32_t)(warp - 2) >> 2;
       const uint32_t h = eg & 1, c0 = (eg >> 1) * 32, lq = (uint32_t)warp & 3;
       const uint32_t row = h * 128 + lq * 32 + lane;
-      const uint64_t pb = ((uint64_t)blockIdx.x * 8 + (row >> 5)) * a.block_stride;
+      const uint64_t pb = (dtile * 8 + (row >> 5)) * a.block_stride;
       const uint64_t doc = pb * 32 + lane;
-      const uint64_t u = (uint64_t)blockIdx.x * kRtM + row;
+      const uint64_t u = dtile * kRtM + row;
       const bool valid = pb < n_blocks && doc < a.n;
       const uint32_t taddr = tmem + ((lq * 32) << 16) + h * kRtAcc1Col;
       // filter list segment of this warp in the dead A stages
@@ -377,7 +381,7 @@ __global__ void __launch_bounds__(kRtThreads, 1)
           const uint32_t pos = S.base[q] + li;
           if (pos < a.cap) {
             a.f_keys[(qb + q) * a.cap + pos] = en.x;
-            const uint64_t rpb = ((uint64_t)blockIdx.x * 8 + (rw >> 5)) * a.block_stride;
+            const uint64_t rpb = (dtile * 8 + (rw >> 5)) * a.block_stride;
             a.f_ids[(qb + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw & 31));
           }
         }
@@ -480,9 +484,10 @@ static void launch_rank_tc(RtArgs a, uint32_t bits, const void* q_split, uint32_
   const uint64_t logical_blocks = (n_blocks + a.block_stride - 1) / a.block_stride;
   const uint64_t doc_tiles = (logical_blocks + 7) / 8;
   const uint64_t q_tiles = (2 * a.nq + a.nt - 1) / a.nt;
-  if (q_tiles > 65535 || doc_tiles > 0x7FFFFFFF || a.n >= (1ull << 32))
+  if (q_tiles * doc_tiles > 0x7FFFFFFFull || a.n >= (1ull << 32))
     throw std::invalid_argument("rank tensor-core scan: grid too large; split the query batch");
-  dim3 grid((unsigned)doc_tiles, (unsigned)q_tiles);
+  a.q_tiles = (uint32_t)q_tiles;
+  dim3 grid((unsigned)(q_tiles * doc_tiles));
 #define OVB_RT(B)                                                                                              \
   do {                                                                                                         \
     OVB_CUDA(cudaFuncSetAttribute(rank_tc_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \

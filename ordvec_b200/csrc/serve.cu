@@ -2,14 +2,20 @@
 // worker threads that each own a CUDA stream and a workspace.
 //
 // Continuous batching: a worker that becomes free takes the oldest pending
-// request and every later pending request with the same (route, k, m), up to
-// max_batch queries, so requests that arrived while other batches ran join
-// the next batch.  Admission: a batch starts only when the device bytes of
-// all batches in flight stay within the HBM budget (a batch larger than the
-// budget runs alone).  Batches of different workers overlap on the device.
-// Each query's result does not depend on its batch-mates (every kernel scores
-// queries independently; stage-1 candidate sets and the rerank are exact per
-// query), so a request gets the same answer alone and in the mix.
+// request and every later pending request of the same route, whatever their
+// k and m, up to max_batch queries, so requests that arrived while other
+// batches ran join the next batch.  A batch runs at its largest k; when its
+// requests' candidate counts differ (m, or the default policy's count for
+// their k) stage 1 selects each query's ordered top-m_max and each query is
+// reranked over its own top-m prefix (engine_two_stage_ragged).  A request
+// then takes the first min(k, m) entries of its rows: the exact top-k of a
+// strict (score, id) order is a prefix of the top-k_max.  Admission: a batch
+// starts only when the device bytes of all batches in flight stay within the
+// HBM budget (a batch larger than the budget runs alone).  Batches of
+// different workers overlap on the device.  Each query's result does not
+// depend on its batch-mates (every kernel scores queries independently;
+// stage-1 candidate sets and the rerank are exact per query), so a request
+// gets the same answer alone and in the mix.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -88,11 +94,24 @@ uint64_t batch_bytes(const Route& r, uint64_t nq, uint64_t k, uint64_t m) {
   return keys + nq * (12 * dim + 24 * me + 24 * k + 8192);
 }
 
+// Candidate count a two-stage request resolves to: its m, or the default
+// policy's count for its k (src/quant.rs:234-262), clamped to n.
+uint64_t resolved_m(const Route& r, const Request& q) {
+  const uint64_t n = r.rq->n;
+  return q.m ? std::min<uint64_t>(q.m, n) : default_candidate_count(q.k, n);
+}
+
 void run_batch(Server& S, const Route& rt, std::vector<ReqPtr>& batch, uint64_t nq, HostBuf& hq, HostBuf& hs,
                HostBuf& hi, DevBuf& dq, DevBuf& ds, DevBuf& di) {
   Workspace& w = workspace();
   const Index& r = *rt.rq;
-  const uint64_t dim = r.dim, k = batch[0]->k, m = batch[0]->m;
+  const uint64_t dim = r.dim;
+  uint64_t k = 0;
+  bool uniform = true;
+  for (auto& q : batch) {
+    k = std::max(k, q->k);
+    uniform = uniform && resolved_m(rt, *q) == resolved_m(rt, *batch[0]);
+  }
   float* hqp = (float*)hq.ensure(nq * dim * 4);
   uint64_t off = 0;
   for (auto& q : batch) {
@@ -101,8 +120,17 @@ void run_batch(Server& S, const Route& rt, std::vector<ReqPtr>& batch, uint64_t 
   }
   float* d_q = (float*)dq.ensure(nq * dim * 4);
   OVB_CUDA(cudaMemcpyAsync(d_q, hqp, nq * dim * 4, cudaMemcpyHostToDevice, w.stream));
-  const uint32_t ke = rt.s1 ? engine_two_stage(r, *rt.s1, d_q, nq, m, k, w, w.stream)
-                            : engine_rankquant_full(r, d_q, nq, k, w, w.stream);
+  uint32_t ke;
+  if (!rt.s1) {
+    ke = engine_rankquant_full(r, d_q, nq, k, w, w.stream);
+  } else if (uniform) {
+    ke = engine_two_stage(r, *rt.s1, d_q, nq, resolved_m(rt, *batch[0]), k, w, w.stream);
+  } else {
+    std::vector<uint64_t> m_of;
+    m_of.reserve(nq);
+    for (auto& q : batch) m_of.insert(m_of.end(), q->nq, resolved_m(rt, *q));
+    ke = engine_two_stage_ragged(r, *rt.s1, d_q, nq, m_of.data(), k, w, w.stream);
+  }
   float* hsp = nullptr;
   int64_t* hip = nullptr;
   if (ke) {
@@ -118,9 +146,16 @@ void run_batch(Server& S, const Route& rt, std::vector<ReqPtr>& batch, uint64_t 
   check_tc_errors(w);
   off = 0;
   for (auto& q : batch) {
-    q->k_out = ke;
-    q->scores.assign(hsp ? hsp + off * ke : hsp, hsp ? hsp + (off + q->nq) * ke : hsp);
-    q->ids.assign(hip ? hip + off * ke : hip, hip ? hip + (off + q->nq) * ke : hip);
+    // this request's own width: min(k, its candidate count), a prefix of each row
+    uint64_t kq = std::min<uint64_t>(q->k, ke);
+    if (rt.s1) kq = std::min<uint64_t>(kq, resolved_m(rt, *q));
+    q->k_out = kq;
+    q->scores.resize(q->nq * kq);
+    q->ids.resize(q->nq * kq);
+    for (uint64_t i = 0; i < q->nq && kq; i++) {
+      std::copy(hsp + (off + i) * ke, hsp + (off + i) * ke + kq, q->scores.begin() + i * kq);
+      std::copy(hip + (off + i) * ke, hip + (off + i) * ke + kq, q->ids.begin() + i * kq);
+    }
     off += q->nq;
   }
 }
@@ -172,12 +207,15 @@ void worker_main(Server* S) {
         continue;
       }
       if (S->pending.empty()) return;  // stopping and drained
-      // the oldest request, then every later one with the same route, k, m
+      // the oldest request, then every later one of the same route
       const ReqPtr head = S->pending.front();
+      uint64_t k_max = 0, m_max = 0;
       for (auto it = S->pending.begin(); it != S->pending.end();) {
         const ReqPtr& q = *it;
-        const bool same = q->route == head->route && q->k == head->k && q->m == head->m;
+        const bool same = q->route == head->route;
         if (same && (batch.empty() || nq + q->nq <= S->max_batch)) {
+          k_max = std::max(k_max, q->k);
+          m_max = std::max(m_max, q->m ? q->m : default_candidate_count(q->k, S->routes[q->route].rq->n));
           nq += q->nq;
           batch.push_back(q);
           it = S->pending.erase(it);
@@ -186,7 +224,7 @@ void worker_main(Server* S) {
         }
       }
       rt = S->routes[head->route];
-      bytes = batch_bytes(rt, nq, head->k, head->m);
+      bytes = batch_bytes(rt, nq, k_max, m_max);
       S->cv_budget.wait(lk, [&] { return S->inflight == 0 || S->inflight + bytes <= S->budget; });
       S->inflight += bytes;
       S->peak_inflight = std::max(S->peak_inflight, S->inflight);

@@ -144,3 +144,29 @@ def test_server_errors():
         t.wait()  # a ticket is collected once
     assert e.value.status == 2
     srv.close()
+
+
+def test_server_batches_mixed_k_and_m_of_one_route():
+    """Requests of one route with different k and candidate counts (explicit m,
+    or the default policy's count for their k) share batches; each request's
+    rows are a prefix of the batch's rows and equal its answer alone."""
+    for rq, s1 in _routes()[1:]:
+        srv = ob.Server(workers=1, max_batch=1024)
+        r = srv.add_route(rq, s1)
+        rng = np.random.default_rng(5)
+        reqs = []
+        for j in range(60):
+            q = ob.synth_queries(300 + j, len(rq), int(rng.choice([1, 3, 8])), rq.dim)[0]
+            k = int(rng.choice([10, 50, 100]))
+            m = 0 if s1 is None else int(rng.choice([0, 0, 400, 1500]))
+            reqs.append((q, k, m))
+        tickets = [srv.submit(r, q, k, m) for q, k, m in reqs]  # all arrive at once
+        got = [t.wait()[0] for t in tickets]
+        st = srv.stats()
+        assert st["requests"] == len(reqs) and st["batches"] < len(reqs) // 4
+        for (q, k, m), g in zip(reqs, got):
+            want = rq.search_asymmetric(q, k) if s1 is None else ob.two_stage_search(rq, s1, q, m, k)
+            assert g.k == want.k
+            assert np.array_equal(g.indices, want.indices)
+            assert np.array_equal(g.scores.view(np.uint32), want.scores.view(np.uint32))
+        srv.close()
