@@ -57,6 +57,8 @@ constexpr int kPEpiWarps = 16;   // warps 6..21: four per TMEM lane quarter
 constexpr int kPThreads = 32 * (2 + kPBuildWarps + kPEpiWarps);
 constexpr int kPEpiThreads = kPEpiWarps * 32;
 constexpr uint32_t kPMaxN = 256;
+constexpr uint32_t kPMaxQ = 1024;        // queries per launch of the pair form (per-query parameters staged once)
+constexpr uint32_t kPRowCacheWords = 16;  // bitmap rows of up to 16 words stay in the builders' registers
 constexpr uint32_t kPKBytes = 128;
 constexpr uint32_t kPTmemCols = 512;
 
@@ -87,6 +89,13 @@ struct PSmem {
   uint32_t qpop[kPMaxN];  // sign bitmaps: query popcounts
   uint32_t cnt[kPMaxN];
   uint32_t base[kPMaxN];
+  // pair form: per-query parameters of the launch (amin, tdoc, thr, qpop, bias, invq)
+  uint32_t qp[PAIR ? 6 * kPMaxQ : 1];
+  uint32_t wamin[PAIR ? kPEpiWarps : 1][64];  // pair form: each epilogue warp's 64 column thresholds
+  // pair form, bitmap rows of <= kPRowCacheWords words: each builder thread's row
+  // of the current doc tile (pitch kPRowCacheWords + 1 words: a warp's 8-byte reads
+  // take the minimum two wavefronts)
+  uint64_t rowc[PAIR ? 128 : 1][kPRowCacheWords + 1];
   uint64_t full_a[PT<PAIR>::kStages];
   uint64_t full_b[PT<PAIR>::kStages];
   uint64_t empty[PT<PAIR>::kStages];
@@ -171,7 +180,42 @@ __device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, %0;" ::"n
 
 struct PairGrid {
   uint32_t n_doc_tiles, q_tiles;
+  uint32_t doc_major;  // 1: a cluster takes whole doc tiles, their query tiles back to back
 };
+
+// The i-th tile of a cluster.  doc_major: doc tiles cluster, cluster +
+// n_clusters, ..., each with its query tiles 0 .. q_tiles-1 in a row, so a doc
+// tile's rows are read once per cluster (the bitmap builders keep them in
+// registers across the query tiles).  Otherwise tiles cluster + i * n_clusters
+// of the doc-major tile order (more clusters busy when there are few doc tiles).
+__device__ __forceinline__ bool tile_at(const PairGrid& g, uint32_t cluster, uint32_t n_clusters, uint64_t i,
+                                        uint64_t& dt, uint32_t& qt) {
+  if (g.doc_major) {
+    dt = cluster + (i / g.q_tiles) * (uint64_t)n_clusters;
+    qt = (uint32_t)(i % g.q_tiles);
+    return dt < g.n_doc_tiles;
+  }
+  const uint64_t tile = cluster + i * (uint64_t)n_clusters;
+  dt = tile / g.q_tiles;
+  qt = (uint32_t)(tile % g.q_tiles);
+  return dt < g.n_doc_tiles;
+}
+
+// tcgen05.ld of 32 columns without the wait (several loads in flight, then tmem_wait)
+__device__ __forceinline__ void tmem_ld32_nw(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+        "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+        "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 template <int MODE, bool PAIR>
 __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs& a, const PairGrid g) {
@@ -185,7 +229,6 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
   const uint32_t rank = PAIR ? cta_rank() : 0u;
   // a "cluster" is a pair of CTAs, or one CTA
   const uint32_t cluster = PAIR ? blockIdx.x >> 1 : blockIdx.x, n_clusters = PAIR ? gridDim.x >> 1 : gridDim.x;
-  const uint64_t total = (uint64_t)g.n_doc_tiles * g.q_tiles;
   const uint32_t nt = a.nt, half = nt / 2;
   const uint32_t n_kb = a.n_kb;
   const uint64_t n_blocks = (a.n + 31) / 32;
@@ -230,8 +273,10 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     // ---- TMA producer (both CTAs) ----------------------------------------------
     if (lane == 0) {
       uint64_t it = 0;  // K-blocks issued
-      for (uint64_t tile = cluster; tile < total && !aborted(S); tile += n_clusters) {
-        const uint64_t q0 = (tile % g.q_tiles) * nt;
+      uint64_t dt_;
+      uint32_t qt_;
+      for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt_, qt_) && !aborted(S); ti++) {
+        const uint64_t q0 = (uint64_t)qt_ * nt;
         for (uint32_t kb = 0; kb < n_kb; kb++, it++) {
           const uint32_t s = (uint32_t)(it % kPStages);
           if (aborted(S)) break;
@@ -260,7 +305,9 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
       uint64_t it = 0, issued = 0;
       uint32_t tcount = 0;
       bool ok = true;
-      for (uint64_t tile = cluster; tile < total && ok; tile += n_clusters, tcount++) {
+      uint64_t dt_;
+      uint32_t qt_;
+      for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt_, qt_) && ok; ti++, tcount++) {
         const uint32_t b = tcount % kBufs;
         if (tcount >= kBufs && !mbar_wait_cluster(&S.acc_empty[b], (tcount / kBufs - 1) & 1)) ok = false;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -334,8 +381,9 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           mbar_arrive(&S.full_a[s]);
       }
     };
-    for (uint64_t tile = cluster; tile < total && ok; tile += n_clusters) {
-      const uint64_t dt = tile / g.q_tiles;
+    uint64_t dt, cached_dt = ~0ull;  // pair form, bitmap rows <= 16 words: doc tile of S.rowc
+    uint32_t qt_;
+    for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt, qt_) && ok; ti++) {
       uint64_t pb[R], doc[R];
       uint32_t a_row[R];  // row offset in a stage: 8-row atoms of 1024 bytes, 128 bytes a row
 #pragma unroll
@@ -344,6 +392,58 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
         pb[i] = (dt * 8 + rank * (kPRows / 32) + (row >> 5)) * a.block_stride;
         doc[i] = pb[i] * 32 + (row & 31);
         a_row[i] = (row >> 3) * 1024 + (row & 7) * 128;
+      }
+      if constexpr (MODE == 1 && PAIR) {
+        if (a.qpv <= kPRowCacheWords) {
+          // the row's words stay in registers while the doc tile's query tiles pass
+          if (dt != cached_dt) {
+            const bool row_ok = pb[0] < n_blocks && doc[0] < a.n;
+            const uint64_t* wp = reinterpret_cast<const uint64_t*>(a.blocks) + (row_ok ? doc[0] : 0) * (uint64_t)a.qpv;
+            // global -> shared without registers; words past the row (or of an
+            // invalid row) are zero-filled (source size 0)
+#pragma unroll
+            for (uint32_t j = 0; j < kPRowCacheWords; j++) {
+              const uint32_t src_bytes = (row_ok && j < a.qpv) ? 8u : 0u;
+              asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_u32(&S.rowc[r][j])),
+                           "l"(wp + (src_bytes ? j : 0)), "r"(src_bytes)
+                           : "memory");
+            }
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            cached_dt = dt;
+            // warm L2 with the row of this cluster's next doc tile
+            const uint64_t nd = dt + n_clusters;
+            if (nd < g.n_doc_tiles) {
+              const uint64_t npb = (nd * 8 + rank * (kPRows / 32) + (r >> 5)) * a.block_stride;
+              const uint64_t ndoc = npb * 32 + (r & 31);
+              if (npb < n_blocks && ndoc < a.n)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const uint64_t*>(a.blocks) +
+                                                             ndoc * (uint64_t)a.qpv));
+            }
+          }
+          const uint32_t base0 = a_row[0], rr = r & 7;
+#pragma unroll
+          for (uint32_t kb = 0; kb < kPRowCacheWords / 2; kb++) {
+            if (kb >= n_kb) break;
+            const uint32_t s = (uint32_t)(it % kPStages);
+            if (!acquire(s)) {
+              ok = false;
+              break;
+            }
+            const uint32_t base = smem_u32(S.a[s]) + base0;
+            const uint64_t w0 = S.rowc[r][2 * kb], w1 = S.rowc[r][2 * kb + 1];
+#pragma unroll
+            for (uint32_t c = 0; c < 8; c++) {  // 16 coordinates per 16-byte chunk
+              const uint32_t h = (uint32_t)((c < 4 ? w0 : w1) >> (16 * (c & 3)));
+              uint32_t o[4];
+#pragma unroll
+              for (uint32_t q = 0; q < 4; q++) o[q] = (((h >> (4 * q)) & 15u) * 0x00204081u) & 0x01010101u;
+              st_shared_v4(base + ((c ^ rr) << 4), o[0], o[1], o[2], o[3]);
+            }
+            publish(s);
+            it++;
+          }
+          continue;
+        }
       }
       if constexpr (MODE == 1) {
         const uint64_t* words[R];
@@ -429,6 +529,181 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
         }
       }
     }
+  } else if constexpr (PAIR) {
+    // ---- epilogue of the pair form: every warp works alone -----------------------
+    // Per-query parameters are staged once per launch (nq <= kPMaxQ); per tile a
+    // warp derives the thresholds of its 64 columns, reads its two 32-column
+    // accumulator chunks (both loads in flight), keeps the passing entries in
+    // its list, releases the accumulator and reserves each entry's slot with a
+    // global atomic: no block barrier per tile.
+    const uint32_t e = (uint32_t)warp - 2 - kPBuildWarps;  // 0..15
+    const uint32_t et = (uint32_t)t - 32 * (2 + kPBuildWarps);
+    const uint32_t lq = (uint32_t)warp & 3;  // TMEM lane quarter (hardware rule: warp % 4)
+    const uint32_t col0 = (e >> 2) * 64;     // this warp's 64 accumulator columns
+    const uint32_t row = lq * 32 + lane;
+    const uint32_t acc_empty0 = peer_addr(smem_u32(&S.acc_empty[0]), 0);
+    // S.qp: [amin | tdoc | thr | qpop | bias | invq] x kPMaxQ
+#define P_am(i) S.qp[(i)]
+#define P_td(i) S.qp[kPMaxQ + (i)]
+#define P_thr(i) S.qp[2 * kPMaxQ + (i)]
+#define P_pop(i) S.qp[3 * kPMaxQ + (i)]
+#define P_bias(i) (*reinterpret_cast<float*>(&S.qp[4 * kPMaxQ + (i)]))
+#define P_invq(i) (*reinterpret_cast<float*>(&S.qp[5 * kPMaxQ + (i)]))
+    for (uint32_t i = et; i < a.nq && i < kPMaxQ; i += kPEpiThreads) {
+      const float bias = MODE == 0 ? a.bias[i] : 0.0f, invq = MODE == 0 ? a.invq[i] : 0.0f;
+      const uint32_t qpop = (MODE == 1 && a.key_kind == 2) ? a.qpop[i] : 0u;
+      uint32_t thr = dense ? 0u : a.thr[i * a.thr_stride], am = 0, td = 0;
+      if (!dense) {
+        if (MODE == 0) {
+          am = filter_amin(bias, invq, a.inv_norm, thr, 255u * a.pairs_pad);
+        } else {
+          am = bm_amin_q(a, qpop, thr);
+          if (a.thr_pos) {  // (key, doc) <= (thr, tdoc): the tie level depends on the tile's doc range
+            const uint32_t p = a.thr_pos[i * a.thr_stride];
+            td = (uint32_t)(((uint64_t)(p >> 5) * a.smp_stride) * 32 + (p & 31));
+            thr = am;
+          }
+        }
+      }
+      P_am(i) = am;
+      P_td(i) = td;
+      P_thr(i) = thr;
+      P_pop(i) = qpop;
+      P_bias(i) = bias;
+      P_invq(i) = invq;
+    }
+    epi_sync();
+    uint32_t* wam = S.wamin[e];
+    uint2* list = S.list[e];
+    uint32_t lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    uint32_t tcount = 0;
+    uint64_t dt;
+    uint32_t qt_;
+    for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt, qt_); ti++, tcount++) {
+      const uint64_t q0 = (uint64_t)qt_ * nt;
+      const uint32_t nqt = (uint32_t)((a.nq - q0) < nt ? (a.nq - q0) : nt);
+      const uint32_t b = tcount % kBufs;
+      const uint64_t first = dt * 256 + rank * kPRows;
+      // thresholds of this warp's columns for this tile
+#pragma unroll
+      for (uint32_t h2 = 0; h2 < 2; h2++) {
+        const uint32_t c = col0 + 32 * h2 + lane;
+        uint32_t am = kNeverPasses;
+        if (c < nqt) {
+          am = P_am(q0 + c);
+          if (MODE == 1 && a.thr_pos && !dense) {
+            const uint32_t td = P_td(q0 + c);
+            am = td >= first + kPRows - 1 ? am : td < first ? am + 1 : kExactCompare;
+          }
+        }
+        wam[32 * h2 + lane] = am;
+      }
+      const bool any_exact = __any_sync(0xFFFFFFFFu, wam[lane] == kExactCompare || wam[32 + lane] == kExactCompare);
+      __syncwarp();
+      bool ready = false;
+      if (lane == 0) ready = !aborted(S) && mbar_wait_cluster(&S.acc_full[b], (tcount / kBufs) & 1);
+      ready = __shfl_sync(0xFFFFFFFFu, ready, 0);
+      if (!ready) {
+        if (lane == 0 && !aborted(S)) raise_abort(S, a.err);
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint64_t pb = (dt * 8 + rank * (kPRows / 32) + (row >> 5)) * a.block_stride;
+      const uint64_t doc = pb * 32 + lane;
+      const uint64_t u = dt * 256 + rank * kPRows + row;
+      const bool valid = pb < n_blocks && doc < a.n;
+      const uint32_t dpop = (MODE == 1 && a.key_kind == 2) ? row_popcount(a, doc, valid) : 0u;
+      const uint32_t taddr = tmem + ((lq * 32) << 16) + b * 256 + col0;
+      const uint32_t nch = col0 >= nt ? 0u : (col0 + 32 >= nt ? 1u : 2u);  // warp-uniform
+      uint32_t wcount = 0;
+      if (nch == 0) {  // nothing to read: release the accumulator at once
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) arrive_remote(acc_empty0 + 8 * b);
+      }
+      for (uint32_t c = 0; c < nch; c++) {
+        const uint32_t cb = col0 + 32 * c;
+        uint32_t v[32];
+        __syncwarp();
+        tmem_ld32(taddr + 32 * c, v);
+        if (c + 1 == nch) {  // the last chunk is in registers: release the accumulator to the MMA
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) arrive_remote(acc_empty0 + 8 * b);
+        }
+        if (MODE == 1 && a.key_kind == 2) {
+#pragma unroll
+          for (uint32_t j = 0; j < 32; j++) v[j] = ham_y(v[j], dpop);
+        }
+        if (dense) {
+#pragma unroll
+          for (uint32_t j = 0; j < 32; j++) {
+            const uint32_t q = cb + j;
+            if (valid && q < nqt)
+              a.keys[(q0 + q) * a.ld + u] = MODE == 0
+                  ? desc_key(tc_score(v[j], P_bias(q0 + q), P_invq(q0 + q), a.inv_norm))
+                  : bm_key_q(a, P_pop(q0 + q), v[j]);
+          }
+          continue;
+        }
+        // column by column: the lanes (docs) passing column j append (acc, column | row << 16)
+        // at ballot-ranked positions of the warp's list
+#pragma unroll
+        for (uint32_t j4 = 0; j4 < 32; j4 += 4) {
+          const uint4 am4 = *reinterpret_cast<const uint4*>(&wam[32 * c + j4]);
+#pragma unroll
+          for (uint32_t jj = 0; jj < 4; jj++) {
+            const uint32_t j = j4 + jj;
+            const uint32_t am = jj == 0 ? am4.x : jj == 1 ? am4.y : jj == 2 ? am4.z : am4.w;
+            bool pass;
+            if (!any_exact || am != kExactCompare) {
+              pass = v[j] >= am;
+            } else {
+              const uint32_t q = q0 + cb + j;
+              if (MODE == 0)
+                pass = desc_key(tc_score(v[j], P_bias(q), P_invq(q), a.inv_norm)) <= P_thr(q);
+              else
+                pass = v[j] > P_thr(q) || (v[j] == P_thr(q) && doc <= P_td(q));
+            }
+            pass = pass && valid;
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, pass);
+            if (bal) {
+              const uint32_t pos = wcount + __popc(bal & lt);
+              if (pass && pos < kPSegCap) list[pos] = make_uint2(v[j], (cb + j) | (row << 16));
+              wcount += __popc(bal);
+            }
+          }
+        }
+      }
+      if (!dense) {
+        __syncwarp();
+        if (wcount > kPSegCap) {  // entries were lost: fail every query of this warp's columns (bit 31 > cap)
+          for (uint32_t j = lane; j < 64; j += 32)
+            if (col0 + j < nqt) atomicOr(&a.cnt[q0 + col0 + j], 0x80000000u);
+        }
+        const uint32_t tot = wcount < kPSegCap ? wcount : kPSegCap;
+        for (uint32_t j = lane; j < tot; j += 32) {
+          const uint2 en = list[j];
+          const uint32_t q = en.y & 0xFFFFu, rw_ = en.y >> 16;
+          const uint32_t pos = atomicAdd(&a.cnt[q0 + q], 1u);
+          if (pos < a.cap) {
+            a.f_keys[(q0 + q) * a.cap + pos] = MODE == 0
+                ? desc_key(tc_score(en.x, P_bias(q0 + q), P_invq(q0 + q), a.inv_norm))
+                : bm_key_q(a, P_pop(q0 + q), en.x);
+            const uint64_t rpb = (dt * 8 + rank * (kPRows / 32) + (rw_ >> 5)) * a.block_stride;
+            a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw_ & 31));
+          }
+        }
+        __syncwarp();  // the list is reused by the next tile
+      }
+    }
+#undef P_am
+#undef P_td
+#undef P_thr
+#undef P_pop
+#undef P_bias
+#undef P_invq
   } else {
     // ---- epilogue (both CTAs) -------------------------------------------------------
     const uint32_t e = (uint32_t)warp - 2 - kPBuildWarps;  // 0..15
@@ -446,8 +721,10 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     uint32_t lt;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
     uint32_t tcount = 0;
-    for (uint64_t tile = cluster; tile < total; tile += n_clusters, tcount++) {
-      const uint64_t dt = tile / g.q_tiles, q0 = (tile % g.q_tiles) * nt;
+    uint64_t dt;
+    uint32_t qt_;
+    for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt, qt_); ti++, tcount++) {
+      const uint64_t q0 = (uint64_t)qt_ * nt;
       const uint32_t nqt = (uint32_t)((a.nq - q0) < nt ? (a.nq - q0) : nt);
       const uint32_t b = tcount % kBufs;
       // per-query parameters of this tile (the previous tile's slot passes are done)
@@ -685,6 +962,26 @@ uint32_t tc_persist_seg_cap() { return PT<false>::kSegCap; }
 template <int MODE>
 void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool pair) {
   if (!a.n || !a.nq) return;
+  if (pair && a.nq > kPMaxQ) {
+    // the pair form stages every query's parameters in shared memory: launch
+    // query chunks of at most kPMaxQ
+    const uint64_t k_bytes = (uint64_t)a.n_kb * kPKBytes;
+    for (uint64_t q0 = 0; q0 < a.nq; q0 += kPMaxQ) {
+      TcArgs c = a;
+      c.nq = a.nq - q0 < kPMaxQ ? a.nq - q0 : kPMaxQ;
+      if (c.qpop) c.qpop += q0;
+      if (c.bias) c.bias += q0;
+      if (c.invq) c.invq += q0;
+      if (c.keys) c.keys += q0 * a.ld;
+      if (c.thr) c.thr += q0 * a.thr_stride;
+      if (c.thr_pos) c.thr_pos += q0 * a.thr_stride;
+      if (c.cnt) c.cnt += q0;
+      if (c.f_keys) c.f_keys += q0 * a.cap;
+      if (c.f_ids) c.f_ids += q0 * a.cap;
+      launch_tc_pair<MODE>(c, b_rows + q0 * k_bytes, stream, pair);
+    }
+    return;
+  }
   const char* what = MODE == 0 ? "FastScan tensor-core scan" : "bitmap tensor-core scan";
   const uint64_t k_bytes = (uint64_t)a.n_kb * kPKBytes;
   if (!a.n_kb || (MODE == 0 && a.n_kb % 4)) throw std::invalid_argument(std::string(what) + ": bad K extent");
@@ -717,6 +1014,8 @@ void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool p
     const size_t smem = sizeof(PSmem<true>) + 1024;
     OVB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     uint64_t clusters = resident_pairs((const void*)kernel, smem);
+    // whole doc tiles per cluster once every cluster gets at least two of them
+    g.doc_major = doc_tiles >= 2 * clusters ? 1u : 0u;
     if (clusters > total) clusters = total;
     kernel<<<(unsigned)(2 * clusters), kPThreads, smem, stream>>>(map, a, g);
   } else {
@@ -727,6 +1026,7 @@ void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool p
     OVB_CUDA(cudaGetDevice(&dev));
     OVB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     uint64_t ctas = (uint64_t)sms;  // one CTA per SM (its shared memory and TMEM fill the SM)
+    g.doc_major = 0;
     if (ctas > total) ctas = total;
     kernel<<<(unsigned)ctas, kPThreads, smem, stream>>>(map, a, g);
   }

@@ -695,6 +695,31 @@ def test_cta_pair_scan_matches_single_cta(monkeypatch, kind):
             assert np.array_equal(got.scores.view(np.uint32), base.scores.view(np.uint32)), key
 
 
+@pytest.mark.parametrize("kind", ["bitmap", "sign"])
+def test_cta_pair_scan_over_query_chunks(monkeypatch, kind):
+    """More than 1,024 queries in one call: the CTA-pair kernel stages every
+    query's parameters in shared memory and runs query chunks of 1,024; its
+    results equal the one-CTA-per-tile kernel's (filter and dense key matrix),
+    on a corpus large enough for whole doc tiles per CTA pair and on one small
+    enough for the interleaved tile order."""
+    for n in (150_000, 9_000):
+        dim = 768
+        docs = ob.synth_docs(73, n, dim)
+        queries, _ = ob.synth_queries(73, n, 1300, dim)
+        ix = ob.Bitmap(dim, 192) if kind == "bitmap" else ob.SignBitmap(dim)
+        ix.add(docs)
+        monkeypatch.setenv("OVB_BITMAP_TC", "1")
+        out = {}
+        for form in ("tile", "pair"):
+            for filt in ("0", "1"):
+                monkeypatch.setenv("OVB_TC_FORM", form)
+                monkeypatch.setenv("OVB_FASTSCAN_FILTER", filt)
+                out[(form, filt)] = np.array(ix.top_m_candidates_batched(queries, 400))
+        base = out[("tile", "0")]
+        for key, got in out.items():
+            assert np.array_equal(got, base), (n, key)
+
+
 @pytest.mark.parametrize("dim,n,nq,m", [(1024, 100_000, 64, 320), (384, 70_001, 300, 700), (192, 40_000, 40, 500)])
 def test_sign_tensor_core_top_m_is_exact(orc, monkeypatch, dim, n, nq, m):
     """Sign-bitmap Hamming candidates from the tensor-core overlap scan
