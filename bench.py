@@ -192,30 +192,32 @@ def split_error_stats(orc, packed, dim, bits, queries, ids, scores):
     return max_abs, max_rel
 
 
-def rerank_report(ob, orc, torch, dev, rq, s1, d_q, queries, m, k, packed, sample, profile_fp64):
-    """The rerank of a two-stage batch: the default (split-BF16 on tcgen05 +
-    FP64 rescoring of the top 2k + 32) against the FP64-table rerank -- stage
-    times of both, and the error against the oracle's FP64 scores of the raw
+def rerank_report(ob, orc, torch, dev, rq, s1, d_q, queries, m, k, packed, sample, profile):
+    """The rerank of a two-stage batch: the split-BF16 tensor-core form
+    (OVB_RERANK_TC=1: tcgen05 contraction + margin test + FP64 rescoring of the
+    top 2k + 32) beside the default FP64-table rerank -- stage times of the
+    split form, and the error against the oracle's FP64 scores of the raw
     split-BF16 scores and of the returned scores, over `sample` queries."""
     nq = d_q.shape[0]
     sp = torch.cuda.current_stream(dev).cuda_stream
     d_s = torch.empty(nq * k, dtype=torch.float32, device=dev)
     d_i = torch.empty(nq * k, dtype=torch.int64, device=dev)
-    out = {"form": "split-BF16 tcgen05 (codes exact in BF16, query hi+lo BF16, f32 accumulation) + margin test + "
-                   "FP64 rescoring of the top 2k+32"}
-    os.environ["OVB_RERANK_TC"] = "0"
+    out = {"default_form": "FP64 per-query nibble tables (CUDA cores)",
+           "split_form": "split-BF16 tcgen05 (codes exact in BF16, query hi+lo BF16, f32 accumulation) + margin test "
+                         "+ FP64 rescoring of the top 2k+32"}
+    os.environ["OVB_RERANK_TC"] = "1"
     try:
-        st = profile_fp64()
+        st = profile()
     finally:
         del os.environ["OVB_RERANK_TC"]
-    out["fp64_rerank_ms"], out["fp64_final_select_ms"] = st[4], st[5]
+    out["split_rerank_ms"], out["split_final_select_ms"] = st[4], st[5]
     if orc is None or packed is None:
         return out
     ob.two_stage_search_device(rq, s1, d_q.data_ptr(), nq, m, k, d_s.data_ptr(), d_i.data_ptr(), sp,
                                rerank="split_raw")
     torch.cuda.synchronize(dev)
     raw_s, raw_i = d_s.view(nq, k).cpu().numpy()[:sample], d_i.view(nq, k).cpu().numpy()[:sample]
-    ob.two_stage_search_device(rq, s1, d_q.data_ptr(), nq, m, k, d_s.data_ptr(), d_i.data_ptr(), sp)
+    ob.two_stage_search_device(rq, s1, d_q.data_ptr(), nq, m, k, d_s.data_ptr(), d_i.data_ptr(), sp, rerank="split")
     torch.cuda.synchronize(dev)
     ex_s, ex_i = d_s.view(nq, k).cpu().numpy()[:sample], d_i.view(nq, k).cpu().numpy()[:sample]
     dim, bits = rq.dim, rq.bits
@@ -519,7 +521,7 @@ def fastscan_run(ob, torch, dev, args, cpu: bool):
             ob, orc, torch, dev, rq, fs, d_q, queries, FS_M, FS_K, packed, 128,
             lambda: ob.two_stage_profile(rq, fs, d_q.data_ptr(), FS_NQ, FS_M, FS_K, d_s.data_ptr(), d_i.data_ptr(),
                                          sp))
-        out["rerank"]["split_rerank_ms"], out["rerank"]["split_final_select_ms"] = st[4], st[5]
+        out["rerank"]["fp64_rerank_ms"], out["rerank"]["fp64_final_select_ms"] = st[4], st[5]
     return out
 
 
@@ -1087,7 +1089,7 @@ def main():
     line["rerank"] = rerank_report(
         ob, orc, torch, dev, rq, bm, d_q, queries, M, K, h_packed, 128,
         lambda: ob.two_stage_profile(rq, bm, d_q.data_ptr(), NQ, M, K, d_s.data_ptr(), d_i.data_ptr(), sp))
-    line["rerank"]["split_rerank_ms"], line["rerank"]["split_final_select_ms"] = stages[4], stages[5]
+    line["rerank"]["fp64_rerank_ms"], line["rerank"]["fp64_final_select_ms"] = stages[4], stages[5]
     if cpu:
         line["codes_identical_to_oracle"] = bool(np.array_equal(bm.payload().view(np.uint64), h_words)
                                                  and np.array_equal(rq.payload(), h_packed))

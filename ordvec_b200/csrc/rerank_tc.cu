@@ -9,8 +9,8 @@
 // Here every (query, 128-candidate tile) is one CTA and the sum is a dense
 // contraction on tcgen05 (kind::f16, f32 accumulation in TMEM):
 //   A (M = 128 rows): the tile's candidate code rows, gathered from HBM into
-//     shared memory by one bulk copy per row (cp.async.bulk, completion on an
-//     mbarrier), then expanded by 8 builder warps (two threads per row) into
+//     shared memory by the builder threads (16-byte cp.async copies spread
+//     over all 256 of them), then expanded by those 8 warps (two threads per row) into
 //     the exact centred codes as bf16 (split_bf16.cuh), 64 coordinates per
 //     128-byte-swizzled K-block, 3 K-block stages;
 //   B (N = 16 rows, TMA): rows 2q .. 2q+15 of the [2 nq x dim] split query
@@ -22,8 +22,8 @@
 // |q|_1 (the same bound as the split-BF16 scan); the engine keeps ids exact
 // by rescoring every candidate within twice that bound of the k-th in FP64.
 //
-// Warp roles: warp 0 gathers the rows and issues the B TMA loads, warp 1
-// issues the MMAs, warps 2..9 build A and then (warps 2..5, one TMEM lane
+// Warp roles: warp 0 issues the B TMA loads, warp 1 issues the MMAs, warps
+// 2..9 gather the rows, build A and then (warps 2..5, one TMEM lane
 // quadrant each) run the epilogue.  Every wait is bounded: a timeout sets
 // *err, drains the copies and MMAs in flight, frees TMEM and returns.
 #include <cuda_bf16.h>
@@ -54,7 +54,6 @@ struct RrSmem {
   uint8_t a[kRrStages][kRrAStage];
   uint8_t b[kRrStages][kRrBStage];
   uint8_t rows[kRrM][kRrRowStride];
-  uint64_t rows_full;
   uint64_t full_a[kRrStages];
   uint64_t full_b[kRrStages];
   uint64_t empty[kRrStages];
@@ -87,12 +86,8 @@ __device__ __forceinline__ bool rr_aborted(const RrSmem& S) {
   return *reinterpret_cast<const volatile uint32_t*>(&S.abort) != 0;
 }
 
-__device__ __forceinline__ void bulk_row(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
+// named barrier 2 over the builder warps
+__device__ __forceinline__ void rr_build_sync() { asm volatile("bar.sync 2, %0;" ::"n"(kRrBuilders) : "memory"); }
 
 __device__ __forceinline__ void tmem_ld2(uint32_t taddr, uint32_t& v0, uint32_t& v1) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(v0), "=r"(v1) : "r"(taddr) : "memory");
@@ -127,7 +122,6 @@ __global__ void __launch_bounds__(kRrThreads, 2)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (t == 32) {
-    mbar_init(&S.rows_full, 1);
     for (int s = 0; s < kRrStages; s++) {
       mbar_init(&S.full_a[s], kRrBuilders / 32);
       mbar_init(&S.full_b[s], 1);
@@ -143,15 +137,6 @@ __global__ void __launch_bounds__(kRrThreads, 2)
   const uint32_t tmem = S.tmem;
 
   if (warp == 0) {
-    // ---- gather the tile's rows (one bulk copy each; ids clamped into range)
-    if (lane == 0) mbar_expect_tx(&S.rows_full, rows * a.bpv);
-    __syncwarp();
-    const uint32_t* ids = a.cands + q * a.ld + j0;
-    for (uint32_t r = lane; r < rows; r += 32) {
-      uint32_t id = __ldg(ids + r);
-      if (id >= a.n) id = (uint32_t)(a.n - 1);
-      bulk_row(S.rows[r], a.codes + (uint64_t)id * a.bpv, a.bpv, &S.rows_full);
-    }
     // ---- B: this query's hi/lo rows (and 14 unread neighbours), one K-block per stage
     if (lane == 0) {
       uint32_t issued = 0;
@@ -169,7 +154,6 @@ __global__ void __launch_bounds__(kRrThreads, 2)
       // drain: no copy may land after the CTA has exited
       for (uint32_t kb = issued > kRrStages ? issued - kRrStages : 0; kb < issued; kb++)
         mbar_wait(&S.full_b[kb % kRrStages], (kb / kRrStages) & 1);
-      mbar_wait(&S.rows_full, 0);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -203,6 +187,21 @@ __global__ void __launch_bounds__(kRrThreads, 2)
     // ---- A builders: row r, coordinates 32 hc .. 32 hc + 31 of each K-block
     const uint32_t bt = (uint32_t)t - 64;
     const uint32_t r = bt & (kRrM - 1), hc = bt >> 7;
+    {
+      // gather the tile's rows: 16-byte copies spread over the builders (ids clamped into range)
+      const uint32_t cpr = a.bpv / 16;  // 16-byte chunks per row
+      const uint32_t* ids = a.cands + q * a.ld + j0;
+      for (uint32_t c = bt; c < rows * cpr; c += kRrBuilders) {
+        const uint32_t rr = c / cpr, part = c - rr * cpr;
+        uint32_t id = __ldg(ids + rr);
+        if (id >= a.n) id = (uint32_t)(a.n - 1);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(S.rows[rr] + 16 * part)),
+                     "l"(a.codes + (uint64_t)id * a.bpv + 16 * part)
+                     : "memory");
+      }
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      rr_build_sync();
+    }
     uint32_t t0, t1;
     nibble_table<BITS>((uint32_t)lane, t0, t1);
     const uint32_t a_row = smem_u32(S.a[0]) + (r >> 3) * 1024 + (r & 7) * 128;
@@ -211,8 +210,7 @@ __global__ void __launch_bounds__(kRrThreads, 2)
     for (uint32_t c = 0; c < 4; c++) dst[c] = a_row + (((4 * hc + c) ^ (r & 7)) << 4);
     // rows past the tile's end are built from row 0 (their scores are not written)
     const uint8_t* src = S.rows[r < rows ? r : 0] + hc * 4 * BITS;
-    bool ok = warp_wait(&S.rows_full, 0, (uint32_t)lane);
-    if (!ok && lane == 0) rr_abort(S, a.err);
+    bool ok = true;
     uint32_t s = 0, par = 0, base = 0;
     for (uint32_t kb = 0; kb < n_kb && ok && !rr_aborted(S); kb++) {
       if (kb >= (uint32_t)kRrStages) {

@@ -68,8 +68,8 @@ constexpr uint32_t kPTmemCols = 512;
 template <bool PAIR>
 struct PT {
   static constexpr uint32_t kRows = PAIR ? 128 : 256;  // doc rows per CTA per tile
-  static constexpr int kStages = PAIR ? 4 : 3;
-  static constexpr uint32_t kSegCap = PAIR ? 256 : 192;  // kept entries per epilogue warp per tile
+  static constexpr int kStages = PAIR ? 5 : 3;
+  static constexpr uint32_t kSegCap = PAIR ? 128 : 192;  // kept entries per epilogue warp per tile
   static constexpr uint32_t kAStage = kRows * kPKBytes;
   static constexpr uint32_t kBStage = (PAIR ? kPMaxN / 2 : kPMaxN) * kPKBytes;
   static constexpr uint32_t kAccBufs = PAIR ? 2 : 1;
@@ -81,16 +81,18 @@ struct PSmem {
   uint8_t a[PT<PAIR>::kStages][PT<PAIR>::kAStage];
   uint8_t b[PT<PAIR>::kStages][PT<PAIR>::kBStage];
   uint2 list[kPEpiWarps][PT<PAIR>::kSegCap];  // (accumulator, q | slot << 8 | row << 16)
-  float bias[kPMaxN];
-  float invq[kPMaxN];
-  uint32_t thr[kPMaxN];
-  uint32_t amin[kPMaxN];
-  uint32_t tdoc[kPMaxN];
-  uint32_t qpop[kPMaxN];  // sign bitmaps: query popcounts
-  uint32_t cnt[kPMaxN];
-  uint32_t base[kPMaxN];
-  // pair form: per-query parameters of the launch (amin, tdoc, thr, qpop, bias, invq)
-  uint32_t qp[PAIR ? 6 * kPMaxQ : 1];
+  // one-CTA form: per-query parameters of the current tile
+  static constexpr uint32_t kTileQ = PAIR ? 1 : kPMaxN;
+  float bias[kTileQ];
+  float invq[kTileQ];
+  uint32_t thr[kTileQ];
+  uint32_t amin[kTileQ];
+  uint32_t tdoc[kTileQ];
+  uint32_t qpop[kTileQ];  // sign bitmaps: query popcounts
+  uint32_t cnt[kTileQ];
+  uint32_t base[kTileQ];
+  // pair form: per-query parameters of the launch, [amin | tdoc or bias | thr | qpop or invq]
+  uint32_t qp[PAIR ? 4 * kPMaxQ : 1];
   uint32_t wamin[PAIR ? kPEpiWarps : 1][64];  // pair form: each epilogue warp's 64 column thresholds
   // pair form, bitmap rows of <= kPRowCacheWords words: each builder thread's row
   // of the current doc tile (pitch kPRowCacheWords + 1 words: a warp's 8-byte reads
@@ -134,6 +136,8 @@ __device__ __forceinline__ void arrive_remote(uint32_t cluster_addr) {
 
 // Barriers with arrivals from the other CTA are waited like local ones.
 __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity) { return mbar_wait(bar, parity); }
+// The MMA issuer's and TMA producer's waits: spinning (no suspend / wake-up latency)
+__device__ __forceinline__ bool mbar_wait_issuer(uint64_t* bar, uint32_t parity) { return mbar_wait_spin(bar, parity); }
 
 template <bool PAIR>
 __device__ __forceinline__ bool aborted(const PSmem<PAIR>& S) {
@@ -280,7 +284,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
         for (uint32_t kb = 0; kb < n_kb; kb++, it++) {
           const uint32_t s = (uint32_t)(it % kPStages);
           if (aborted(S)) break;
-          if (it >= (uint64_t)kPStages && !mbar_wait(&S.empty[s], (uint32_t)((it / kPStages - 1) & 1))) {
+          if (it >= (uint64_t)kPStages && !mbar_wait_issuer(&S.empty[s], (uint32_t)((it / kPStages - 1) & 1))) {
             raise_abort(S, a.err);
             break;
           }
@@ -309,12 +313,12 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
       uint32_t qt_;
       for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt_, qt_) && ok; ti++, tcount++) {
         const uint32_t b = tcount % kBufs;
-        if (tcount >= kBufs && !mbar_wait_cluster(&S.acc_empty[b], (tcount / kBufs - 1) & 1)) ok = false;
+        if (tcount >= kBufs && !mbar_wait_issuer(&S.acc_empty[b], (tcount / kBufs - 1) & 1)) ok = false;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + b * 256;
         for (uint32_t kb = 0; kb < n_kb && ok; kb++, it++) {
           const uint32_t s = (uint32_t)(it % kPStages), par = (uint32_t)((it / kPStages) & 1);
-          if (aborted(S) || !mbar_wait_cluster(&S.full_b[s], par) || !mbar_wait_cluster(&S.full_a[s], par)) {
+          if (aborted(S) || !mbar_wait_issuer(&S.full_b[s], par) || !mbar_wait_issuer(&S.full_a[s], par)) {
             ok = false;
             break;
           }
@@ -542,13 +546,13 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     const uint32_t col0 = (e >> 2) * 64;     // this warp's 64 accumulator columns
     const uint32_t row = lq * 32 + lane;
     const uint32_t acc_empty0 = peer_addr(smem_u32(&S.acc_empty[0]), 0);
-    // S.qp: [amin | tdoc | thr | qpop | bias | invq] x kPMaxQ
+    // S.qp: [amin | tdoc (bitmap) or bias (FastScan) | thr | qpop (bitmap) or invq (FastScan)] x kPMaxQ
 #define P_am(i) S.qp[(i)]
 #define P_td(i) S.qp[kPMaxQ + (i)]
 #define P_thr(i) S.qp[2 * kPMaxQ + (i)]
 #define P_pop(i) S.qp[3 * kPMaxQ + (i)]
-#define P_bias(i) (*reinterpret_cast<float*>(&S.qp[4 * kPMaxQ + (i)]))
-#define P_invq(i) (*reinterpret_cast<float*>(&S.qp[5 * kPMaxQ + (i)]))
+#define P_bias(i) (*reinterpret_cast<float*>(&S.qp[kPMaxQ + (i)]))
+#define P_invq(i) (*reinterpret_cast<float*>(&S.qp[3 * kPMaxQ + (i)]))
     for (uint32_t i = et; i < a.nq && i < kPMaxQ; i += kPEpiThreads) {
       const float bias = MODE == 0 ? a.bias[i] : 0.0f, invq = MODE == 0 ? a.invq[i] : 0.0f;
       const uint32_t qpop = (MODE == 1 && a.key_kind == 2) ? a.qpop[i] : 0u;
@@ -566,11 +570,14 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
         }
       }
       P_am(i) = am;
-      P_td(i) = td;
       P_thr(i) = thr;
-      P_pop(i) = qpop;
-      P_bias(i) = bias;
-      P_invq(i) = invq;
+      if (MODE == 0) {
+        P_bias(i) = bias;
+        P_invq(i) = invq;
+      } else {
+        P_td(i) = td;
+        P_pop(i) = qpop;
+      }
     }
     epi_sync();
     uint32_t* wam = S.wamin[e];
@@ -647,33 +654,51 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           }
           continue;
         }
-        // column by column: the lanes (docs) passing column j append (acc, column | row << 16)
-        // at ballot-ranked positions of the warp's list
+        uint32_t hm = 0;  // the columns (queries) this lane's doc passes
+        if (!any_exact) {
 #pragma unroll
-        for (uint32_t j4 = 0; j4 < 32; j4 += 4) {
-          const uint4 am4 = *reinterpret_cast<const uint4*>(&wam[32 * c + j4]);
-#pragma unroll
-          for (uint32_t jj = 0; jj < 4; jj++) {
-            const uint32_t j = j4 + jj;
-            const uint32_t am = jj == 0 ? am4.x : jj == 1 ? am4.y : jj == 2 ? am4.z : am4.w;
-            bool pass;
-            if (!any_exact || am != kExactCompare) {
-              pass = v[j] >= am;
-            } else {
-              const uint32_t q = q0 + cb + j;
-              if (MODE == 0)
-                pass = desc_key(tc_score(v[j], P_bias(q), P_invq(q), a.inv_norm)) <= P_thr(q);
-              else
-                pass = v[j] > P_thr(q) || (v[j] == P_thr(q) && doc <= P_td(q));
-            }
-            pass = pass && valid;
-            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, pass);
-            if (bal) {
-              const uint32_t pos = wcount + __popc(bal & lt);
-              if (pass && pos < kPSegCap) list[pos] = make_uint2(v[j], (cb + j) | (row << 16));
-              wcount += __popc(bal);
-            }
+          for (uint32_t j = 0; j < 32; j += 4) {
+            const uint4 am = *reinterpret_cast<const uint4*>(&wam[32 * c + j]);
+            hm |= ((uint32_t)(v[j] >= am.x) << j) | ((uint32_t)(v[j + 1] >= am.y) << (j + 1)) |
+                  ((uint32_t)(v[j + 2] >= am.z) << (j + 2)) | ((uint32_t)(v[j + 3] >= am.w) << (j + 3));
           }
+        } else {
+#pragma unroll
+          for (uint32_t j = 0; j < 32; j++) {
+            const uint32_t q = q0 + cb + j;
+            const uint32_t am = wam[32 * c + j];
+            bool pass;
+            if (am != kExactCompare)
+              pass = v[j] >= am;
+            else if (MODE == 0)
+              pass = desc_key(tc_score(v[j], P_bias(q), P_invq(q), a.inv_norm)) <= P_thr(q);
+            else
+              pass = v[j] > P_thr(q) || (v[j] == P_thr(q) && doc <= P_td(q));
+            hm |= (uint32_t)pass << j;
+          }
+        }
+        if (!valid) hm = 0;
+        while (__any_sync(0xFFFFFFFFu, hm != 0)) {
+          const bool has = hm != 0;
+          const uint32_t j = has ? (uint32_t)(__ffs(hm) - 1) : 0u;
+          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+          const uint32_t pos = wcount + __popc(bal & lt);
+          if (has && pos < kPSegCap) {
+            // v[j] by a 5-level select tree on the bits of j
+            uint32_t t16[16], t8[8], t4[4], t2[2];
+#pragma unroll
+            for (uint32_t i = 0; i < 16; i++) t16[i] = (j & 1) ? v[2 * i + 1] : v[2 * i];
+#pragma unroll
+            for (uint32_t i = 0; i < 8; i++) t8[i] = (j & 2) ? t16[2 * i + 1] : t16[2 * i];
+#pragma unroll
+            for (uint32_t i = 0; i < 4; i++) t4[i] = (j & 4) ? t8[2 * i + 1] : t8[2 * i];
+#pragma unroll
+            for (uint32_t i = 0; i < 2; i++) t2[i] = (j & 8) ? t4[2 * i + 1] : t4[2 * i];
+            const uint32_t acc = (j & 16) ? t2[1] : t2[0];
+            list[pos] = make_uint2(acc, (cb + j) | (row << 16));
+          }
+          wcount += __popc(bal);
+          hm &= hm - 1;
         }
       }
       if (!dense) {

@@ -79,6 +79,33 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
+// Non-blocking poll (no suspend): for the single issuing threads (MMA, TMA),
+// whose waits sit on the critical path; a suspended waiter pays a wake-up.
+__device__ __forceinline__ bool mbar_test(uint32_t addr, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(addr), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded spinning parity wait: at most 2^26 polls and about kWaitNs of wall
+// time (the clock is read every 1024 polls); returns false on timeout.
+__device__ __forceinline__ bool mbar_wait_spin(uint64_t* bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  if (mbar_test(addr, parity)) return true;
+  uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < (1u << 26); it++) {
+    if (mbar_test(addr, parity)) return true;
+    if ((it & 1023) == 1023 && global_ns() - t0 > kWaitNs) return false;
+  }
+  return false;
+}
+
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
