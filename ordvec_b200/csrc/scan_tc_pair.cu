@@ -68,7 +68,10 @@ constexpr uint32_t kPTmemCols = 512;
 template <bool PAIR>
 struct PT {
   static constexpr uint32_t kRows = PAIR ? 128 : 256;  // doc rows per CTA per tile
-  static constexpr int kStages = PAIR ? 5 : 3;
+  // A: K-block slots (pair form: a bitmap doc tile's whole row when it fits,
+  // built once and read by all its query tiles; otherwise a ring); B: a ring
+  static constexpr int kASlots = PAIR ? 6 : 3;
+  static constexpr int kBStages = PAIR ? 4 : 3;
   static constexpr uint32_t kSegCap = PAIR ? 128 : 192;  // kept entries per epilogue warp per tile
   static constexpr uint32_t kAStage = kRows * kPKBytes;
   static constexpr uint32_t kBStage = (PAIR ? kPMaxN / 2 : kPMaxN) * kPKBytes;
@@ -78,8 +81,8 @@ struct PT {
 
 template <bool PAIR>
 struct PSmem {
-  uint8_t a[PT<PAIR>::kStages][PT<PAIR>::kAStage];
-  uint8_t b[PT<PAIR>::kStages][PT<PAIR>::kBStage];
+  uint8_t a[PT<PAIR>::kASlots][PT<PAIR>::kAStage];
+  uint8_t b[PT<PAIR>::kBStages][PT<PAIR>::kBStage];
   uint2 list[kPEpiWarps][PT<PAIR>::kSegCap];  // (accumulator, q | slot << 8 | row << 16)
   // one-CTA form: per-query parameters of the current tile
   static constexpr uint32_t kTileQ = PAIR ? 1 : kPMaxN;
@@ -98,9 +101,10 @@ struct PSmem {
   // of the current doc tile (pitch kPRowCacheWords + 1 words: a warp's 8-byte reads
   // take the minimum two wavefronts)
   uint64_t rowc[PAIR ? 128 : 1][kPRowCacheWords + 1];
-  uint64_t full_a[PT<PAIR>::kStages];
-  uint64_t full_b[PT<PAIR>::kStages];
-  uint64_t empty[PT<PAIR>::kStages];
+  uint64_t full_a[PT<PAIR>::kASlots];
+  uint64_t empty_a[PT<PAIR>::kASlots];
+  uint64_t full_b[PT<PAIR>::kBStages];
+  uint64_t empty_b[PT<PAIR>::kBStages];
   uint64_t acc_full[2];
   uint64_t acc_empty[2];
   uint32_t tmem;
@@ -136,7 +140,7 @@ __device__ __forceinline__ void arrive_remote(uint32_t cluster_addr) {
 
 // Barriers with arrivals from the other CTA are waited like local ones.
 __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity) { return mbar_wait(bar, parity); }
-// The MMA issuer's and TMA producer's waits: spinning (no suspend / wake-up latency)
+// The MMA issuer's waits: short suspend hints (it sits on the critical path)
 __device__ __forceinline__ bool mbar_wait_issuer(uint64_t* bar, uint32_t parity) { return mbar_wait_spin(bar, parity); }
 
 template <bool PAIR>
@@ -224,7 +228,7 @@ __device__ __forceinline__ void tmem_wait() { asm volatile("tcgen05.wait::ld.syn
 template <int MODE, bool PAIR>
 __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs& a, const PairGrid g) {
   using T = PT<PAIR>;
-  constexpr int kPStages = T::kStages;
+  constexpr int kASlots = T::kASlots, kBStages = T::kBStages;
   constexpr uint32_t kPRows = T::kRows, kPSegCap = T::kSegCap, kBufs = T::kAccBufs;
   extern __shared__ uint8_t smem_raw[];
   PSmem<PAIR>& S =
@@ -237,12 +241,18 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
   const uint32_t n_kb = a.n_kb;
   const uint64_t n_blocks = (a.n + 31) / 32;
   const bool dense = a.keys != nullptr;
+  // A resident per doc tile: built once, read by the doc tile's q_tiles
+  // consecutive tiles (whole doc tiles per cluster, rows of <= 12 words)
+  const bool resA = PAIR && MODE == 1 && g.doc_major && n_kb <= (uint32_t)kASlots && a.qpv <= kPRowCacheWords;
 
   if (t == 32) {
-    for (int s = 0; s < kPStages; s++) {
+    for (int s = 0; s < kASlots; s++) {
       mbar_init(&S.full_a[s], (PAIR ? 2 : 1) * kPBuildWarps);  // builder warps of both CTAs
-      mbar_init(&S.full_b[s], 1);                              // the leader's expect_tx
-      mbar_init(&S.empty[s], 1);                               // the leader's MMA commit
+      mbar_init(&S.empty_a[s], 1);                             // the leader's MMA commit
+    }
+    for (int s = 0; s < kBStages; s++) {
+      mbar_init(&S.full_b[s], 1);   // the leader's expect_tx
+      mbar_init(&S.empty_b[s], 1);  // the leader's MMA commit
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&S.acc_full[b], 1);
@@ -282,9 +292,9 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
       for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt_, qt_) && !aborted(S); ti++) {
         const uint64_t q0 = (uint64_t)qt_ * nt;
         for (uint32_t kb = 0; kb < n_kb; kb++, it++) {
-          const uint32_t s = (uint32_t)(it % kPStages);
+          const uint32_t s = (uint32_t)(it % kBStages);
           if (aborted(S)) break;
-          if (it >= (uint64_t)kPStages && !mbar_wait_issuer(&S.empty[s], (uint32_t)((it / kPStages - 1) & 1))) {
+          if (it >= (uint64_t)kBStages && !mbar_wait(&S.empty_b[s], (uint32_t)((it / kBStages - 1) & 1))) {
             raise_abort(S, a.err);
             break;
           }
@@ -298,38 +308,47 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
       }
       // the leader waits (bounded) until its last copies, and the peer's, landed
       if (rank == 0)
-        for (uint64_t j = it > (uint64_t)kPStages ? it - kPStages : 0; j < it; j++)
-          mbar_wait_cluster(&S.full_b[j % kPStages], (uint32_t)((j / kPStages) & 1));
+        for (uint64_t j = it > (uint64_t)kBStages ? it - kBStages : 0; j < it; j++)
+          mbar_wait_cluster(&S.full_b[j % kBStages], (uint32_t)((j / kBStages) & 1));
     }
   } else if (warp == 1) {
     // ---- MMA issuer (leader) ------------------------------------------------------
     if (lane == 0 && rank == 0) {
       // D s32, A/B u8, K-major, N = nt; M = 256 across the pair, or two M = 128 halves
       const uint32_t idesc = (2u << 4) | ((nt >> 3) << 17) | ((uint32_t)((PAIR ? 256 : 128) >> 4) << 24);
-      uint64_t it = 0, issued = 0;
+      uint64_t it = 0, ita = 0, issued = 0;  // B K-blocks, A ring K-blocks, last issued B K-block + 1
       uint32_t tcount = 0;
       bool ok = true;
       uint64_t dt_;
       uint32_t qt_;
       for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt_, qt_) && ok; ti++, tcount++) {
         const uint32_t b = tcount % kBufs;
+        const uint32_t pa_res = (uint32_t)((ti / g.q_tiles) & 1);  // resident A: phase of this doc tile
+        const bool last_q = qt_ + 1 == g.q_tiles;                  // resident A: its last reader
         if (tcount >= kBufs && !mbar_wait_issuer(&S.acc_empty[b], (tcount / kBufs - 1) & 1)) ok = false;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + b * 256;
         for (uint32_t kb = 0; kb < n_kb && ok; kb++, it++) {
-          const uint32_t s = (uint32_t)(it % kPStages), par = (uint32_t)((it / kPStages) & 1);
-          if (aborted(S) || !mbar_wait_issuer(&S.full_b[s], par) || !mbar_wait_issuer(&S.full_a[s], par)) {
+          const uint32_t sb = (uint32_t)(it % kBStages), pb = (uint32_t)((it / kBStages) & 1);
+          const uint32_t sa = resA ? kb : (uint32_t)(ita % kASlots);
+          const uint32_t pa = resA ? pa_res : (uint32_t)((ita / kASlots) & 1);
+          if (aborted(S) || !mbar_wait_issuer(&S.full_b[sb], pb) || !mbar_wait_issuer(&S.full_a[sa], pa)) {
             ok = false;
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint32_t a0 = smem_u32(S.a[s]), b0 = smem_u32(S.b[s]);
+          const uint32_t a0 = smem_u32(S.a[sa]), b0 = smem_u32(S.b[sb]);
+          const bool free_a = !resA || last_q;
           if (PAIR) {
 #pragma unroll
             for (uint32_t j = 0; j < 4; j++)
               mma_i8_pair(d, sw128_desc(a0 + 32 * j), sw128_desc(b0 + 32 * j), idesc, (kb | j) != 0);
-            commit_pair(smem_u32(&S.empty[s]));
-            commit_pair(peer_addr(smem_u32(&S.empty[s]), 1));
+            commit_pair(smem_u32(&S.empty_b[sb]));
+            commit_pair(peer_addr(smem_u32(&S.empty_b[sb]), 1));
+            if (free_a) {
+              commit_pair(smem_u32(&S.empty_a[sa]));
+              commit_pair(peer_addr(smem_u32(&S.empty_a[sa]), 1));
+            }
           } else {
 #pragma unroll
             for (uint32_t j = 0; j < 4; j++) {
@@ -337,8 +356,10 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
               mma_i8(d, sw128_desc(a0 + 32 * j), bd, idesc, (kb | j) != 0);
               mma_i8(d + 256, sw128_desc(a0 + kPRows / 2 * kPKBytes + 32 * j), bd, idesc, (kb | j) != 0);
             }
-            mma_commit(&S.empty[s]);
+            mma_commit(&S.empty_b[sb]);
+            mma_commit(&S.empty_a[sa]);
           }
+          if (!resA) ita++;
           issued = it + 1;
         }
         if (!ok) break;
@@ -353,7 +374,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
         if (!aborted(S)) raise_abort(S, a.err);
         // no MMA in flight when the pair frees its tensor memory
         if (issued > 0)
-          mbar_wait(&S.empty[(issued - 1) % kPStages], (uint32_t)(((issued - 1) / kPStages) & 1));
+          mbar_wait(&S.empty_b[(issued - 1) % kBStages], (uint32_t)(((issued - 1) / kBStages) & 1));
       }
     }
   } else if (warp < 2 + kPBuildWarps) {
@@ -364,11 +385,11 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     const uint32_t full_a0 = PAIR ? peer_addr(smem_u32(&S.full_a[0]), 0) : 0u;
     uint64_t it = 0;
     bool ok = true;
-    // wait for stage s to be free, or stop (warp-uniform)
+    // wait for A ring slot s to be free, or stop (warp-uniform)
     auto acquire = [&](uint32_t s) -> bool {
       bool w = true;
-      if (it >= (uint64_t)kPStages) {
-        if (lane == 0) w = !aborted(S) && mbar_wait(&S.empty[s], (uint32_t)((it / kPStages - 1) & 1));
+      if (it >= (uint64_t)kASlots) {
+        if (lane == 0) w = !aborted(S) && mbar_wait(&S.empty_a[s], (uint32_t)((it / kASlots - 1) & 1));
         w = __shfl_sync(0xFFFFFFFFu, w, 0);
         if (!w && lane == 0 && !aborted(S)) raise_abort(S, a.err);
         __syncwarp();
@@ -424,14 +445,32 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
                                                              ndoc * (uint64_t)a.qpv));
             }
           }
+          if (resA && qt_ != 0) continue;  // the doc tile's A is resident: built at its first query tile
+          const uint64_t dc = ti / g.q_tiles;  // resident A: doc tiles this cluster started before
           const uint32_t base0 = a_row[0], rr = r & 7;
 #pragma unroll
           for (uint32_t kb = 0; kb < kPRowCacheWords / 2; kb++) {
             if (kb >= n_kb) break;
-            const uint32_t s = (uint32_t)(it % kPStages);
-            if (!acquire(s)) {
-              ok = false;
-              break;
+            uint32_t s;
+            if (resA) {
+              s = kb;
+              if (dc > 0) {  // the previous doc tile's last query tile has read this slot
+                bool w = true;
+                if (lane == 0) w = !aborted(S) && mbar_wait(&S.empty_a[s], (uint32_t)((dc - 1) & 1));
+                w = __shfl_sync(0xFFFFFFFFu, w, 0);
+                if (!w && lane == 0 && !aborted(S)) raise_abort(S, a.err);
+                __syncwarp();
+                if (!w) {
+                  ok = false;
+                  break;
+                }
+              }
+            } else {
+              s = (uint32_t)(it % kASlots);
+              if (!acquire(s)) {
+                ok = false;
+                break;
+              }
             }
             const uint32_t base = smem_u32(S.a[s]) + base0;
             const uint64_t w0 = S.rowc[r][2 * kb], w1 = S.rowc[r][2 * kb + 1];
@@ -472,7 +511,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
             w[i][2] = (row_ok[i] && wi < a.qpv) ? __ldg(words[i] + wi) : 0ull;
             w[i][3] = (row_ok[i] && wi + 1 < a.qpv) ? __ldg(words[i] + wi + 1) : 0ull;
           }
-          const uint32_t s = (uint32_t)(it % kPStages);
+          const uint32_t s = (uint32_t)(it % kASlots);
           if (!acquire(s)) {
             ok = false;
             break;
@@ -512,7 +551,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           }
 #pragma unroll
           for (uint32_t j = 0; j < 4; j++) {
-            const uint32_t s = (uint32_t)(it % kPStages);
+            const uint32_t s = (uint32_t)(it % kASlots);
             if (!acquire(s)) {
               ok = false;
               break;

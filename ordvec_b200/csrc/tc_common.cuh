@@ -93,15 +93,29 @@ __device__ __forceinline__ bool mbar_test(uint32_t addr, uint32_t parity) {
   return done != 0;
 }
 
-// Bounded spinning parity wait: at most 2^26 polls and about kWaitNs of wall
-// time (the clock is read every 1024 polls); returns false on timeout.
+// Bounded parity wait for a single issuing thread on the critical path: polls
+// with a short suspend hint (the thread is woken within ~kShortSuspendNs, not
+// after the long hint of mbar_wait), at most 2^24 polls and about kWaitNs of
+// wall time; returns false on timeout.
+constexpr uint32_t kShortSuspendNs = 64;
+__device__ __forceinline__ bool mbar_try_short(uint32_t addr, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(addr), "r"(parity), "n"(kShortSuspendNs)
+      : "memory");
+  return done != 0;
+}
 __device__ __forceinline__ bool mbar_wait_spin(uint64_t* bar, uint32_t parity) {
   const uint32_t addr = smem_u32(bar);
   if (mbar_test(addr, parity)) return true;
   uint64_t t0 = global_ns();
-  for (uint32_t it = 0; it < (1u << 26); it++) {
-    if (mbar_test(addr, parity)) return true;
-    if ((it & 1023) == 1023 && global_ns() - t0 > kWaitNs) return false;
+  for (uint32_t it = 0; it < (1u << 24); it++) {
+    if (mbar_try_short(addr, parity)) return true;
+    if ((it & 255) == 255 && global_ns() - t0 > kWaitNs) return false;
   }
   return false;
 }
