@@ -191,39 +191,43 @@ struct PairGrid {
   uint32_t doc_major;  // 1: a cluster takes whole doc tiles, their query tiles back to back
 };
 
-// The i-th tile of a cluster.  doc_major: doc tiles cluster, cluster +
+// A cluster's walk over its tiles.  doc_major: doc tiles cluster, cluster +
 // n_clusters, ..., each with its query tiles 0 .. q_tiles-1 in a row, so a doc
-// tile's rows are read once per cluster (the bitmap builders keep them in
-// registers across the query tiles).  Otherwise tiles cluster + i * n_clusters
-// of the doc-major tile order (more clusters busy when there are few doc tiles).
-__device__ __forceinline__ bool tile_at(const PairGrid& g, uint32_t cluster, uint32_t n_clusters, uint64_t i,
-                                        uint64_t& dt, uint32_t& qt) {
-  if (g.doc_major) {
-    dt = cluster + (i / g.q_tiles) * (uint64_t)n_clusters;
-    qt = (uint32_t)(i % g.q_tiles);
-    return dt < g.n_doc_tiles;
+// tile's rows are read once per cluster (the bitmap builders build its A once
+// for all its query tiles).  Otherwise tiles cluster + i * n_clusters of the
+// doc-major tile order (more clusters busy when there are few doc tiles).  The
+// doc-major walk advances without divisions (the issuing threads run it once
+// per tile on their critical path); di counts the doc tiles walked before dt.
+// The host keeps doc tiles x query tiles below 2^32.
+struct TileCursor {
+  uint32_t dt, qt, di, tile;
+  __device__ __forceinline__ void start(const PairGrid& g, uint32_t cluster) {
+    di = 0;
+    tile = cluster;
+    if (g.doc_major) {
+      dt = cluster;
+      qt = 0;
+    } else {
+      dt = tile / g.q_tiles;
+      qt = tile - dt * g.q_tiles;
+    }
   }
-  const uint64_t tile = cluster + i * (uint64_t)n_clusters;
-  dt = tile / g.q_tiles;
-  qt = (uint32_t)(tile % g.q_tiles);
-  return dt < g.n_doc_tiles;
-}
+  __device__ __forceinline__ bool valid(const PairGrid& g) const { return dt < g.n_doc_tiles; }
+  __device__ __forceinline__ void next(const PairGrid& g, uint32_t n_clusters) {
+    if (g.doc_major) {
+      if (++qt == g.q_tiles) {
+        qt = 0;
+        dt += n_clusters;
+        di++;
+      }
+    } else {
+      tile += n_clusters;
+      dt = tile / g.q_tiles;
+      qt = tile - dt * g.q_tiles;
+    }
+  }
+};
 
-// tcgen05.ld of 32 columns without the wait (several loads in flight, then tmem_wait)
-__device__ __forceinline__ void tmem_ld32_nw(uint32_t taddr, uint32_t (&v)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
-        "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
-        "=r"(v[30]), "=r"(v[31])
-      : "r"(taddr)
-      : "memory");
-}
-__device__ __forceinline__ void tmem_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 template <int MODE, bool PAIR>
 __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs& a, const PairGrid g) {
@@ -287,10 +291,9 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     // ---- TMA producer (both CTAs) ----------------------------------------------
     if (lane == 0) {
       uint64_t it = 0;  // K-blocks issued
-      uint64_t dt_;
-      uint32_t qt_;
-      for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt_, qt_) && !aborted(S); ti++) {
-        const uint64_t q0 = (uint64_t)qt_ * nt;
+      TileCursor tc_;
+      for (tc_.start(g, cluster); tc_.valid(g) && !aborted(S); tc_.next(g, n_clusters)) {
+        const uint64_t q0 = (uint64_t)tc_.qt * nt;
         for (uint32_t kb = 0; kb < n_kb; kb++, it++) {
           const uint32_t s = (uint32_t)(it % kBStages);
           if (aborted(S)) break;
@@ -319,12 +322,11 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
       uint64_t it = 0, ita = 0, issued = 0;  // B K-blocks, A ring K-blocks, last issued B K-block + 1
       uint32_t tcount = 0;
       bool ok = true;
-      uint64_t dt_;
-      uint32_t qt_;
-      for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt_, qt_) && ok; ti++, tcount++) {
+      TileCursor tc_;
+      for (tc_.start(g, cluster); tc_.valid(g) && ok; tc_.next(g, n_clusters), tcount++) {
         const uint32_t b = tcount % kBufs;
-        const uint32_t pa_res = (uint32_t)((ti / g.q_tiles) & 1);  // resident A: phase of this doc tile
-        const bool last_q = qt_ + 1 == g.q_tiles;                  // resident A: its last reader
+        const uint32_t pa_res = tc_.di & 1;            // resident A: phase of this doc tile
+        const bool last_q = tc_.qt + 1 == g.q_tiles;  // resident A: its last reader
         if (tcount >= kBufs && !mbar_wait_issuer(&S.acc_empty[b], (tcount / kBufs - 1) & 1)) ok = false;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + b * 256;
@@ -406,9 +408,11 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           mbar_arrive(&S.full_a[s]);
       }
     };
-    uint64_t dt, cached_dt = ~0ull;  // pair form, bitmap rows <= 16 words: doc tile of S.rowc
-    uint32_t qt_;
-    for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt, qt_) && ok; ti++) {
+    uint64_t cached_dt = ~0ull;  // pair form, bitmap rows <= 16 words: doc tile of S.rowc
+    TileCursor tc_;
+    for (tc_.start(g, cluster); tc_.valid(g) && ok; tc_.next(g, n_clusters)) {
+      const uint64_t dt = tc_.dt;
+      const uint32_t qt_ = tc_.qt;
       uint64_t pb[R], doc[R];
       uint32_t a_row[R];  // row offset in a stage: 8-row atoms of 1024 bytes, 128 bytes a row
 #pragma unroll
@@ -446,7 +450,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
             }
           }
           if (resA && qt_ != 0) continue;  // the doc tile's A is resident: built at its first query tile
-          const uint64_t dc = ti / g.q_tiles;  // resident A: doc tiles this cluster started before
+          const uint64_t dc = tc_.di;  // resident A: doc tiles this cluster started before
           const uint32_t base0 = a_row[0], rr = r & 7;
 #pragma unroll
           for (uint32_t kb = 0; kb < kPRowCacheWords / 2; kb++) {
@@ -624,9 +628,10 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     uint32_t lt;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
     uint32_t tcount = 0;
-    uint64_t dt;
-    uint32_t qt_;
-    for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt, qt_); ti++, tcount++) {
+    TileCursor tc_;
+    for (tc_.start(g, cluster); tc_.valid(g); tc_.next(g, n_clusters), tcount++) {
+      const uint64_t dt = tc_.dt;
+      const uint32_t qt_ = tc_.qt;
       const uint64_t q0 = (uint64_t)qt_ * nt;
       const uint32_t nqt = (uint32_t)((a.nq - q0) < nt ? (a.nq - q0) : nt);
       const uint32_t b = tcount % kBufs;
@@ -785,9 +790,10 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     uint32_t lt;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
     uint32_t tcount = 0;
-    uint64_t dt;
-    uint32_t qt_;
-    for (uint64_t ti = 0; tile_at(g, cluster, n_clusters, ti, dt, qt_); ti++, tcount++) {
+    TileCursor tc_;
+    for (tc_.start(g, cluster); tc_.valid(g); tc_.next(g, n_clusters), tcount++) {
+      const uint64_t dt = tc_.dt;
+      const uint32_t qt_ = tc_.qt;
       const uint64_t q0 = (uint64_t)qt_ * nt;
       const uint32_t nqt = (uint32_t)((a.nq - q0) < nt ? (a.nq - q0) : nt);
       const uint32_t b = tcount % kBufs;
@@ -1068,8 +1074,8 @@ void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool p
   PairGrid g;
   const uint64_t doc_tiles = (logical_blocks + 7) / 8;
   const uint64_t q_tiles = (a.nq + a.nt - 1) / a.nt;
-  if (doc_tiles > 0xFFFFFFFFull || q_tiles > 0xFFFFFFFFull || a.n >= (1ull << 32))
-    throw std::invalid_argument(std::string(what) + ": too many tiles");
+  if (doc_tiles * q_tiles + 2048 > 0xFFFFFFFFull || a.n >= (1ull << 32))
+    throw std::invalid_argument(std::string(what) + ": too many tiles; split the query batch");
   g.n_doc_tiles = (uint32_t)doc_tiles;
   g.q_tiles = (uint32_t)q_tiles;
   const uint64_t total = doc_tiles * q_tiles;
