@@ -140,7 +140,8 @@ __device__ __forceinline__ void arrive_remote(uint32_t cluster_addr) {
 
 // Barriers with arrivals from the other CTA are waited like local ones.
 __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity) { return mbar_wait(bar, parity); }
-// The MMA issuer's waits: short suspend hints (it sits on the critical path)
+// Waits of the threads that feed or issue the MMAs: short suspend hints (a
+// waiter suspended for long wakes late and the tensor pipe idles meanwhile)
 __device__ __forceinline__ bool mbar_wait_issuer(uint64_t* bar, uint32_t parity) { return mbar_wait_spin(bar, parity); }
 
 template <bool PAIR>
@@ -297,7 +298,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
         for (uint32_t kb = 0; kb < n_kb; kb++, it++) {
           const uint32_t s = (uint32_t)(it % kBStages);
           if (aborted(S)) break;
-          if (it >= (uint64_t)kBStages && !mbar_wait(&S.empty_b[s], (uint32_t)((it / kBStages - 1) & 1))) {
+          if (it >= (uint64_t)kBStages && !mbar_wait_issuer(&S.empty_b[s], (uint32_t)((it / kBStages - 1) & 1))) {
             raise_abort(S, a.err);
             break;
           }
@@ -319,7 +320,8 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     if (lane == 0 && rank == 0) {
       // D s32, A/B u8, K-major, N = nt; M = 256 across the pair, or two M = 128 halves
       const uint32_t idesc = (2u << 4) | ((nt >> 3) << 17) | ((uint32_t)((PAIR ? 256 : 128) >> 4) << 24);
-      uint64_t it = 0, ita = 0, issued = 0;  // B K-blocks, A ring K-blocks, last issued B K-block + 1
+      uint64_t it = 0, issued = 0;  // B K-blocks issued, last issued B K-block + 1
+      uint32_t rb_s = 0, rb_p = 0, ra_s = 0, ra_p = 0;  // B ring / A ring: slot and phase of the next K-block
       uint32_t tcount = 0;
       bool ok = true;
       TileCursor tc_;
@@ -331,9 +333,9 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + b * 256;
         for (uint32_t kb = 0; kb < n_kb && ok; kb++, it++) {
-          const uint32_t sb = (uint32_t)(it % kBStages), pb = (uint32_t)((it / kBStages) & 1);
-          const uint32_t sa = resA ? kb : (uint32_t)(ita % kASlots);
-          const uint32_t pa = resA ? pa_res : (uint32_t)((ita / kASlots) & 1);
+          const uint32_t sb = rb_s, pb = rb_p;
+          const uint32_t sa = resA ? kb : ra_s;
+          const uint32_t pa = resA ? pa_res : ra_p;
           if (aborted(S) || !mbar_wait_issuer(&S.full_b[sb], pb) || !mbar_wait_issuer(&S.full_a[sa], pa)) {
             ok = false;
             break;
@@ -342,9 +344,10 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           const uint32_t a0 = smem_u32(S.a[sa]), b0 = smem_u32(S.b[sb]);
           const bool free_a = !resA || last_q;
           if (PAIR) {
+            // a 32-byte K step adds 2 to the descriptor's start-address field (16-byte units)
+            const uint64_t ad = sw128_desc(a0), bd = sw128_desc(b0);
 #pragma unroll
-            for (uint32_t j = 0; j < 4; j++)
-              mma_i8_pair(d, sw128_desc(a0 + 32 * j), sw128_desc(b0 + 32 * j), idesc, (kb | j) != 0);
+            for (uint32_t j = 0; j < 4; j++) mma_i8_pair(d, ad + 2 * j, bd + 2 * j, idesc, (kb | j) != 0);
             commit_pair(smem_u32(&S.empty_b[sb]));
             commit_pair(peer_addr(smem_u32(&S.empty_b[sb]), 1));
             if (free_a) {
@@ -361,7 +364,14 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
             mma_commit(&S.empty_b[sb]);
             mma_commit(&S.empty_a[sa]);
           }
-          if (!resA) ita++;
+          if (!resA && ++ra_s == (uint32_t)kASlots) {
+            ra_s = 0;
+            ra_p ^= 1;
+          }
+          if (++rb_s == (uint32_t)kBStages) {
+            rb_s = 0;
+            rb_p ^= 1;
+          }
           issued = it + 1;
         }
         if (!ok) break;
@@ -391,7 +401,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     auto acquire = [&](uint32_t s) -> bool {
       bool w = true;
       if (it >= (uint64_t)kASlots) {
-        if (lane == 0) w = !aborted(S) && mbar_wait(&S.empty_a[s], (uint32_t)((it / kASlots - 1) & 1));
+        if (lane == 0) w = !aborted(S) && mbar_wait_issuer(&S.empty_a[s], (uint32_t)((it / kASlots - 1) & 1));
         w = __shfl_sync(0xFFFFFFFFu, w, 0);
         if (!w && lane == 0 && !aborted(S)) raise_abort(S, a.err);
         __syncwarp();
@@ -460,7 +470,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
               s = kb;
               if (dc > 0) {  // the previous doc tile's last query tile has read this slot
                 bool w = true;
-                if (lane == 0) w = !aborted(S) && mbar_wait(&S.empty_a[s], (uint32_t)((dc - 1) & 1));
+                if (lane == 0) w = !aborted(S) && mbar_wait_issuer(&S.empty_a[s], (uint32_t)((dc - 1) & 1));
                 w = __shfl_sync(0xFFFFFFFFu, w, 0);
                 if (!w && lane == 0 && !aborted(S)) raise_abort(S, a.err);
                 __syncwarp();
