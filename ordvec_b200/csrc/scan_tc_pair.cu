@@ -178,10 +178,16 @@ __device__ __forceinline__ void mma_i8_pair(uint32_t d_tmem, uint64_t a_desc, ui
       : "memory");
 }
 
-// Arrive-one on the barrier at cluster address `bar` when every MMA this
-// thread issued so far has completed.
-__device__ __forceinline__ void commit_pair(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+
+// Arrive-one on the barrier at the same shared-memory offset in both CTAs of
+// the pair when every MMA this thread issued so far has completed (a commit
+// with a CTA mask: one instruction for both CTAs' barriers).
+__device__ __forceinline__ void commit_both(uint32_t local_bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          local_bar),
+      "h"((uint16_t)3)
+      : "memory");
 }
 
 // named barrier 1 over the epilogue warps
@@ -348,12 +354,8 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
             const uint64_t ad = sw128_desc(a0), bd = sw128_desc(b0);
 #pragma unroll
             for (uint32_t j = 0; j < 4; j++) mma_i8_pair(d, ad + 2 * j, bd + 2 * j, idesc, (kb | j) != 0);
-            commit_pair(smem_u32(&S.empty_b[sb]));
-            commit_pair(peer_addr(smem_u32(&S.empty_b[sb]), 1));
-            if (free_a) {
-              commit_pair(smem_u32(&S.empty_a[sa]));
-              commit_pair(peer_addr(smem_u32(&S.empty_a[sa]), 1));
-            }
+            commit_both(smem_u32(&S.empty_b[sb]));
+            if (free_a) commit_both(smem_u32(&S.empty_a[sa]));
           } else {
 #pragma unroll
             for (uint32_t j = 0; j < 4; j++) {
@@ -376,8 +378,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
         }
         if (!ok) break;
         if (PAIR) {
-          commit_pair(smem_u32(&S.acc_full[b]));
-          commit_pair(peer_addr(smem_u32(&S.acc_full[b]), 1));
+          commit_both(smem_u32(&S.acc_full[b]));
         } else {
           mma_commit(&S.acc_full[b]);
         }
