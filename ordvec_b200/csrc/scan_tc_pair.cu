@@ -342,7 +342,11 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           const uint32_t sb = rb_s, pb = rb_p;
           const uint32_t sa = resA ? kb : ra_s;
           const uint32_t pa = resA ? pa_res : ra_p;
-          if (aborted(S) || !mbar_wait_issuer(&S.full_b[sb], pb) || !mbar_wait_issuer(&S.full_a[sa], pa)) {
+          // resident A: after the doc tile's first query tile its slots are known
+          // full (nothing refills them before its last query tile frees them)
+          const bool need_a = !resA || tc_.qt == 0;
+          if ((kb == 0 && aborted(S)) || !mbar_wait_issuer(&S.full_b[sb], pb) ||
+              (need_a && !mbar_wait_issuer(&S.full_a[sa], pa))) {
             ok = false;
             break;
           }
