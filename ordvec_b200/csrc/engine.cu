@@ -188,6 +188,10 @@ void bitmap_tc_candidates(const Index& s1, const uint64_t* qb, uint32_t qpv, uin
   uint32_t* qpop = key_kind == 2 ? (uint32_t*)w.bias.ensure(nq * 4) : nullptr;  // bias is FastScan's
   launch_bitmap_tc_query(qb, nq, qpv, qx, qpop, st);
   const uint64_t* words = s1.codes.as<uint64_t>();
+  // the filter's query operand on the FP4 tensor cores, built with the int8 one
+  // (the sample scan writes every key and stays on int8)
+  const uint64_t row4 = (uint64_t)bitmap_fp4_kblocks(qpv) * 128;
+  uint8_t* q4 = nullptr;
   uint32_t* err = w.tc_err_word(st);
   auto dense = [&](uint64_t qa, uint64_t qn) {
     full_scan_select(w, qn, n, me, key_bits, sk + qa * me, si + qa * me, st,
@@ -202,6 +206,10 @@ void bitmap_tc_candidates(const Index& s1, const uint64_t* qb, uint32_t qpv, uin
     dense(0, nq);
     return;
   }
+  if (bitmap_fp4_usable(qpv)) {
+    q4 = (uint8_t*)w.q_nib.ensure(nq * row4);
+    launch_bitmap_fp4_query(qb, nq, qpv, q4, st);
+  }
   filtered_select(
       w, n, nq, me, fp, key_bits, sk, si, st,
       [&](uint64_t q0, uint64_t qn, uint32_t* smp) {
@@ -210,8 +218,9 @@ void bitmap_tc_candidates(const Index& s1, const uint64_t* qb, uint32_t qpv, uin
       },
       [&](uint64_t q0, uint64_t qn, const uint32_t* thr, const uint32_t* pos, uint32_t* cnt, uint32_t* fk,
           uint32_t* fi) {
-        launch_bitmap_filter_tc(words, n, qpv, key_kind, s1.n_top, qpop ? qpop + q0 : nullptr, qx + q0 * row, qn, thr,
-                                pos, fp.stride, fp.r, cnt, fp.cap, fk, fi, err, st);
+        launch_bitmap_filter_tc(words, n, qpv, key_kind, s1.n_top, qpop ? qpop + q0 : nullptr, qx + q0 * row,
+                                q4 ? q4 + q0 * row4 : nullptr, qn, thr, pos, fp.stride, fp.r, cnt, fp.cap, fk, fi, err,
+                                st);
       },
       dense);
 }

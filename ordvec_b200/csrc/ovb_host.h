@@ -102,6 +102,8 @@ struct Workspace {
   DevBuf smp_keys, thr_keys, thr_ids, f_keys, f_ids, f_cnt, f_flag;
   // split-BF16 rank scan: [hi; lo] query rows and |q|_1
   DevBuf q_split, q_l1;
+  // bitmap filter on FP4 tensor cores: the query bits as e2m1 nibbles
+  DevBuf q_nib;
   // split-BF16 rerank: top-kp split keys / ids per query, their FP64 keys, the margin flag
   DevBuf rr_keys, rr_ids, rr_keys2, rr_flag;
   HostBuf rr_flag_host;

@@ -95,13 +95,23 @@ void launch_bitmap_tc_query(const uint64_t* qbits, uint64_t nq, uint32_t qpv, ui
 void launch_bitmap_scan_tc(const uint64_t* words, uint64_t n, uint32_t qpv, uint32_t key_kind, uint32_t n_top,
                            const uint32_t* qpop, const uint8_t* q_bytes, uint64_t nq, uint32_t block_stride,
                            uint32_t* keys, uint64_t ld, uint32_t* err, cudaStream_t stream);
+// The same scan on FP4 tensor cores (kind::mxf4): the query operand is the
+// query bits as packed e2m1 nibbles (launch_bitmap_fp4_query),
+// bitmap_fp4_kblocks(qpv) * 128 bytes per query; bitmap_fp4_usable(qpv) says
+// whether the filter below may take it (OVB_BITMAP_FP4=0 says no).
+uint32_t bitmap_fp4_kblocks(uint32_t qpv);
+bool bitmap_fp4_usable(uint32_t qpv);
+void launch_bitmap_fp4_query(const uint64_t* qbits, uint64_t nq, uint32_t qpv, uint8_t* out, cudaStream_t stream);
 // Filter with a tie bound: keeps (key32, doc) <= (thr, tdoc) in (key, doc)
 // order, tdoc = the doc of sample position thr_pos[q * thr_stride] of a sample
 // taken with block stride smp_stride (every doc at key < thr when thr_pos is null).
+// With q_nib (the FP4 query operand) it runs on the FP4 tensor cores, else on
+// int8 ones with q_bytes; same results.
 void launch_bitmap_filter_tc(const uint64_t* words, uint64_t n, uint32_t qpv, uint32_t key_kind, uint32_t n_top,
-                             const uint32_t* qpop, const uint8_t* q_bytes, uint64_t nq, const uint32_t* thr, const uint32_t* thr_pos,
-                             uint32_t smp_stride, uint64_t thr_stride, uint32_t* cnt, uint32_t cap, uint32_t* f_keys,
-                             uint32_t* f_ids, uint32_t* err, cudaStream_t stream);
+                             const uint32_t* qpop, const uint8_t* q_bytes, const uint8_t* q_nib, uint64_t nq,
+                             const uint32_t* thr, const uint32_t* thr_pos, uint32_t smp_stride, uint64_t thr_stride,
+                             uint32_t* cnt, uint32_t cap, uint32_t* f_keys, uint32_t* f_ids, uint32_t* err,
+                             cudaStream_t stream);
 // *flag |= 1 when some cnt[q] < need or > cap.
 void launch_filter_check(const uint32_t* cnt, uint64_t nq, uint32_t need, uint32_t cap, uint32_t* flag,
                          cudaStream_t stream);

@@ -521,6 +521,24 @@ __global__ void expand_query_bits_kernel(const uint64_t* __restrict__ qbits, uin
   }
 }
 
+// query bits -> packed e2m1 nibbles (byte j: coordinate 2 j in the low nibble,
+// 2 j + 1 in the high one; 0b0010 = 1.0 where the bit is set), row_bytes per query
+__global__ void expand_query_nibbles_kernel(const uint64_t* __restrict__ qbits, uint64_t nq, uint32_t qpv,
+                                            uint32_t row_bytes, uint8_t* __restrict__ out) {
+  const uint64_t total = nq * (uint64_t)row_bytes;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t q = t / row_bytes;
+    const uint32_t j = (uint32_t)(t % row_bytes);
+    uint32_t v = 0;
+    if (j / 32 < qpv) {
+      const uint32_t two = (uint32_t)(qbits[q * qpv + j / 32] >> ((2 * j) % 64)) & 3u;
+      v = ((two & 1u) ? 0x02u : 0u) | ((two & 2u) ? 0x20u : 0u);
+    }
+    out[t] = (uint8_t)v;
+  }
+}
+
 __global__ void filter_check_kernel(const uint32_t* __restrict__ cnt, uint64_t nq, uint32_t need, uint32_t cap,
                                     uint32_t* __restrict__ flag) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -636,6 +654,24 @@ void launch_fastscan_filter_tc(const uint8_t* blocks, uint64_t n, uint32_t pairs
 }
 
 uint32_t bitmap_tc_kblocks(uint32_t qpv) { return (qpv + 1) / 2; }
+uint32_t bitmap_fp4_kblocks(uint32_t qpv) { return (qpv + 3) / 4; }
+
+// The bitmap filter runs on the FP4 tensor cores when its rows fit the FP4
+// form and the bitmap family runs on CTA pairs; OVB_BITMAP_FP4=0 keeps int8.
+bool bitmap_fp4_usable(uint32_t qpv) {
+  const char* e = getenv("OVB_BITMAP_FP4");
+  if (e && e[0] == '0') return false;
+  return qpv >= 1 && qpv <= tc_fp4_max_words() && tc_form(1) == TcForm::kPair;
+}
+
+void launch_bitmap_fp4_query(const uint64_t* qbits, uint64_t nq, uint32_t qpv, uint8_t* out, cudaStream_t stream) {
+  if (!nq) return;
+  const uint32_t row = bitmap_fp4_kblocks(qpv) * kTcKBytes;
+  uint64_t blocks = (nq * row + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  expand_query_nibbles_kernel<<<(unsigned)blocks, 256, 0, stream>>>(qbits, nq, qpv, row, out);
+  launched();
+}
 
 void launch_bitmap_tc_query(const uint64_t* qbits, uint64_t nq, uint32_t qpv, uint8_t* out, uint32_t* qpop,
                             cudaStream_t stream) {
@@ -672,10 +708,10 @@ void launch_bitmap_scan_tc(const uint64_t* words, uint64_t n, uint32_t qpv, uint
 }
 
 void launch_bitmap_filter_tc(const uint64_t* words, uint64_t n, uint32_t qpv, uint32_t key_kind, uint32_t n_top,
-                           const uint32_t* qpop,
-                             const uint8_t* q_bytes, uint64_t nq, const uint32_t* thr, const uint32_t* thr_pos,
-                             uint32_t smp_stride, uint64_t thr_stride, uint32_t* cnt, uint32_t cap, uint32_t* f_keys,
-                             uint32_t* f_ids, uint32_t* err, cudaStream_t stream) {
+                             const uint32_t* qpop, const uint8_t* q_bytes, const uint8_t* q_nib, uint64_t nq,
+                             const uint32_t* thr, const uint32_t* thr_pos, uint32_t smp_stride, uint64_t thr_stride,
+                             uint32_t* cnt, uint32_t cap, uint32_t* f_keys, uint32_t* f_ids, uint32_t* err,
+                             cudaStream_t stream) {
   TcArgs a{};
   a.blocks = reinterpret_cast<const uint8_t*>(words);
   a.n = n;
@@ -695,6 +731,12 @@ void launch_bitmap_filter_tc(const uint64_t* words, uint64_t n, uint32_t qpv, ui
   a.f_keys = f_keys;
   a.f_ids = f_ids;
   a.err = err;
+  if (q_nib) {
+    if (!bitmap_fp4_usable(qpv)) throw std::invalid_argument("bitmap FP4 filter: rows too long for the FP4 form");
+    a.n_kb = bitmap_fp4_kblocks(qpv);
+    launch_tc_pair<2>(a, q_nib, stream, true);
+    return;
+  }
   launch_tc<1>(a, q_bytes, stream);
 }
 

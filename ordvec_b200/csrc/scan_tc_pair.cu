@@ -35,6 +35,16 @@
 //
 // Results are the one-CTA kernel's (scan_fastscan_tc.cu), bit for bit: same
 // integer accumulators, same key functions and filter rules.
+//
+// The bitmap filter also runs on the FP4 tensor cores (MODE 2): a set bit is
+// the e2m1 value 1.0 (nibble 0b0010), a clear one 0, so an MMA of K=64 packed
+// nibbles (kind::mxf4, every ue8m0 block scale 1) sums 64 products of 0/1 into
+// an f32 accumulator, exact for overlaps below 2^24, at twice the int8 rate and
+// with half the operand bytes.  The scale factors sit in tensor-memory columns
+// [224, 256) (A) and [480, 512) (B), all bytes 127, past the two accumulators
+// of N <= 224 query columns; non-negative f32 values order like their bit
+// patterns, so the epilogue compares the accumulator bits with the f32 bits of
+// each query's integer threshold.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -61,6 +71,9 @@ constexpr uint32_t kPMaxQ = 1024;        // queries per launch of the pair form 
 constexpr uint32_t kPRowCacheWords = 16;  // bitmap rows of up to 16 words stay in the builders' registers
 constexpr uint32_t kPKBytes = 128;
 constexpr uint32_t kPTmemCols = 512;
+constexpr uint32_t kPF4MaxN = 224;                  // FP4 form: query columns per tile (scale factors above)
+constexpr uint32_t kSfaCol = 224, kSfbCol = 480;    // FP4 form: scale-factor columns of A and B
+constexpr uint32_t kUnitScales = 0x7F7F7F7Fu;       // four ue8m0 bytes of 2^0
 
 // PAIR: CTA pairs, 128 doc rows per CTA, two 256-column accumulators.
 // !PAIR: one CTA per SM, 256 doc rows (two M=128 halves) in one 512-column
@@ -179,6 +192,45 @@ __device__ __forceinline__ void mma_i8_pair(uint32_t d_tmem, uint64_t a_desc, ui
 }
 
 
+// tcgen05.mma kind::mxf4 across the pair: packed e2m1 A and B, f32 D, one
+// ue8m0 scale per 32 K-elements of each row read from tensor memory at sfa /
+// sfb; one K=64 step (32 bytes of each row).
+__device__ __forceinline__ void mma_mxf4_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                              uint32_t accumulate, uint32_t sfa, uint32_t sfb) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%5], [%6], p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(sfa), "r"(sfb)
+      : "memory");
+}
+
+// Stores the word w into 32 consecutive columns from taddr in every lane of the
+// calling warp's tensor-memory lane quarter.
+__device__ __forceinline__ void tmem_fill32(uint32_t taddr, uint32_t w) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr),
+      "r"(w)
+      : "memory");
+}
+
+// Bits 0..7 of x -> eight nibbles, nibble i = e2m1 1.0 (0b0010) where bit i is
+// set and 0 elsewhere (bit i moves to bit 4 i + 1; the shifted copies never
+// overlap, so no carries).
+__device__ __forceinline__ uint32_t fp4_ones8(uint32_t x) {
+  uint32_t v = x & 0xFFu;
+  v = (v | (v << 12)) & 0x000F000Fu;
+  v = (v | (v << 6)) & 0x03030303u;
+  v = (v | (v << 3)) & 0x11111111u;
+  return v << 1;
+}
+
+// The integer value of an f32 accumulator holding an integer in [0, 2^23)
+// (add 2^23: the integer lands in the mantissa bits).
+__device__ __forceinline__ uint32_t f4_int(uint32_t bits) {
+  return __float_as_uint(__fadd_rn(__uint_as_float(bits), 8388608.0f)) & 0x7FFFFFu;
+}
+
 // Arrive-one on the barrier at the same shared-memory offset in both CTAs of
 // the pair when every MMA this thread issued so far has completed (a commit
 // with a CTA mask: one instruction for both CTAs' barriers).
@@ -239,6 +291,8 @@ struct TileCursor {
 template <int MODE, bool PAIR>
 __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs& a, const PairGrid g) {
   using T = PT<PAIR>;
+  constexpr bool BM = MODE != 0, F4 = MODE == 2;  // bitmap rows; on the FP4 tensor cores
+  static_assert(!F4 || PAIR, "the FP4 bitmap form runs on CTA pairs");
   constexpr int kASlots = T::kASlots, kBStages = T::kBStages;
   constexpr uint32_t kPRows = T::kRows, kPSegCap = T::kSegCap, kBufs = T::kAccBufs;
   extern __shared__ uint8_t smem_raw[];
@@ -252,9 +306,15 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
   const uint32_t n_kb = a.n_kb;
   const uint64_t n_blocks = (a.n + 31) / 32;
   const bool dense = a.keys != nullptr;
+  // FP4 form: filter only, rows held in the builders' row cache (host-checked;
+  // a launch that breaks either does no work and sets bit 0 of *err)
+  if (F4 && (dense || a.qpv > kPRowCacheWords || nt > kPF4MaxN)) {
+    if (t == 0 && blockIdx.x == 0) atomicOr(a.err, 1u);
+    return;
+  }
   // A resident per doc tile: built once, read by the doc tile's q_tiles
   // consecutive tiles (whole doc tiles per cluster, rows of <= 12 words)
-  const bool resA = PAIR && MODE == 1 && g.doc_major && n_kb <= (uint32_t)kASlots && a.qpv <= kPRowCacheWords;
+  const bool resA = PAIR && BM && g.doc_major && n_kb <= (uint32_t)kASlots && a.qpv <= kPRowCacheWords;
 
   if (t == 32) {
     for (int s = 0; s < kASlots; s++) {
@@ -293,6 +353,19 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = S.tmem;
+  if constexpr (F4) {
+    // unit scale factors in both CTAs before the first MMA: one epilogue warp
+    // per tensor-memory lane quarter (warp % 4)
+    if (warp >= 2 + kPBuildWarps && warp < 6 + kPBuildWarps) {
+      const uint32_t lanes = ((uint32_t)(warp & 3) * 32) << 16;
+      tmem_fill32(tmem + lanes + kSfaCol, kUnitScales);
+      tmem_fill32(tmem + lanes + kSfbCol, kUnitScales);
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    cluster_sync_all();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
 
   if (warp == 0) {
     // ---- TMA producer (both CTAs) ----------------------------------------------
@@ -324,8 +397,10 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
   } else if (warp == 1) {
     // ---- MMA issuer (leader) ------------------------------------------------------
     if (lane == 0 && rank == 0) {
-      // D s32, A/B u8, K-major, N = nt; M = 256 across the pair, or two M = 128 halves
-      const uint32_t idesc = (2u << 4) | ((nt >> 3) << 17) | ((uint32_t)((PAIR ? 256 : 128) >> 4) << 24);
+      // i8: D s32, A/B u8, K-major, N = nt; M = 256 across the pair, or two M = 128 halves.
+      // FP4: A/B e2m1 (format 1), K-major, ue8m0 scales (bit 23), scale ids 0, K = 64, D f32
+      const uint32_t idesc = F4 ? (1u << 7) | (1u << 10) | ((nt >> 3) << 17) | (1u << 23) | (16u << 24)
+                                : (2u << 4) | ((nt >> 3) << 17) | ((uint32_t)((PAIR ? 256 : 128) >> 4) << 24);
       uint64_t it = 0, issued = 0;  // B K-blocks issued, last issued B K-block + 1
       uint32_t rb_s = 0, rb_p = 0, ra_s = 0, ra_p = 0;  // B ring / A ring: slot and phase of the next K-block
       uint32_t tcount = 0;
@@ -356,8 +431,14 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           if (PAIR) {
             // a 32-byte K step adds 2 to the descriptor's start-address field (16-byte units)
             const uint64_t ad = sw128_desc(a0), bd = sw128_desc(b0);
+            if constexpr (F4) {
 #pragma unroll
-            for (uint32_t j = 0; j < 4; j++) mma_i8_pair(d, ad + 2 * j, bd + 2 * j, idesc, (kb | j) != 0);
+              for (uint32_t j = 0; j < 4; j++)
+                mma_mxf4_pair(d, ad + 2 * j, bd + 2 * j, idesc, (kb | j) != 0, tmem + kSfaCol, tmem + kSfbCol);
+            } else {
+#pragma unroll
+              for (uint32_t j = 0; j < 4; j++) mma_i8_pair(d, ad + 2 * j, bd + 2 * j, idesc, (kb | j) != 0);
+            }
             commit_both(smem_u32(&S.empty_b[sb]));
             if (free_a) commit_both(smem_u32(&S.empty_a[sa]));
           } else {
@@ -437,7 +518,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
         doc[i] = pb[i] * 32 + (row & 31);
         a_row[i] = (row >> 3) * 1024 + (row & 7) * 128;
       }
-      if constexpr (MODE == 1 && PAIR) {
+      if constexpr (BM && PAIR) {
         if (a.qpv <= kPRowCacheWords) {
           // the row's words stay in registers while the doc tile's query tiles pass
           if (dt != cached_dt) {
@@ -467,8 +548,9 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           if (resA && qt_ != 0) continue;  // the doc tile's A is resident: built at its first query tile
           const uint64_t dc = tc_.di;  // resident A: doc tiles this cluster started before
           const uint32_t base0 = a_row[0], rr = r & 7;
+          constexpr uint32_t kWordsPerKb = F4 ? 4 : 2;  // 128 bytes: 256 nibbles or 128 bytes of 0/1
 #pragma unroll
-          for (uint32_t kb = 0; kb < kPRowCacheWords / 2; kb++) {
+          for (uint32_t kb = 0; kb < kPRowCacheWords / kWordsPerKb; kb++) {
             if (kb >= n_kb) break;
             uint32_t s;
             if (resA) {
@@ -492,14 +574,23 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
               }
             }
             const uint32_t base = smem_u32(S.a[s]) + base0;
-            const uint64_t w0 = S.rowc[r][2 * kb], w1 = S.rowc[r][2 * kb + 1];
+            if constexpr (F4) {
 #pragma unroll
-            for (uint32_t c = 0; c < 8; c++) {  // 16 coordinates per 16-byte chunk
-              const uint32_t h = (uint32_t)((c < 4 ? w0 : w1) >> (16 * (c & 3)));
-              uint32_t o[4];
+              for (uint32_t c = 0; c < 8; c++) {  // 32 coordinates (half a word) per 16-byte chunk
+                const uint32_t h = (uint32_t)(S.rowc[r][4 * kb + (c >> 1)] >> (32 * (c & 1)));
+                st_shared_v4(base + ((c ^ rr) << 4), fp4_ones8(h), fp4_ones8(h >> 8), fp4_ones8(h >> 16),
+                             fp4_ones8(h >> 24));
+              }
+            } else {
+              const uint64_t w0 = S.rowc[r][2 * kb], w1 = S.rowc[r][2 * kb + 1];
 #pragma unroll
-              for (uint32_t q = 0; q < 4; q++) o[q] = (((h >> (4 * q)) & 15u) * 0x00204081u) & 0x01010101u;
-              st_shared_v4(base + ((c ^ rr) << 4), o[0], o[1], o[2], o[3]);
+              for (uint32_t c = 0; c < 8; c++) {  // 16 coordinates per 16-byte chunk
+                const uint32_t h = (uint32_t)((c < 4 ? w0 : w1) >> (16 * (c & 3)));
+                uint32_t o[4];
+#pragma unroll
+                for (uint32_t q = 0; q < 4; q++) o[q] = (((h >> (4 * q)) & 15u) * 0x00204081u) & 0x01010101u;
+                st_shared_v4(base + ((c ^ rr) << 4), o[0], o[1], o[2], o[3]);
+              }
             }
             publish(s);
             it++;
@@ -550,7 +641,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           }
           publish(s);
         }
-      } else {
+      } else if constexpr (MODE == 0) {
         const uint8_t* row_codes[R];
         bool row_valid[R];
         uint4 next[R];
@@ -613,7 +704,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
 #define P_invq(i) (*reinterpret_cast<float*>(&S.qp[3 * kPMaxQ + (i)]))
     for (uint32_t i = et; i < a.nq && i < kPMaxQ; i += kPEpiThreads) {
       const float bias = MODE == 0 ? a.bias[i] : 0.0f, invq = MODE == 0 ? a.invq[i] : 0.0f;
-      const uint32_t qpop = (MODE == 1 && a.key_kind == 2) ? a.qpop[i] : 0u;
+      const uint32_t qpop = (BM && a.key_kind == 2) ? a.qpop[i] : 0u;
       uint32_t thr = dense ? 0u : a.thr[i * a.thr_stride], am = 0, td = 0;
       if (!dense) {
         if (MODE == 0) {
@@ -640,6 +731,9 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     epi_sync();
     uint32_t* wam = S.wamin[e];
     uint2* list = S.list[e];
+    // FP4 form: accumulators are f32 bits (compared as bits) except for sign
+    // bitmaps, whose epilogue transform needs the integer
+    const bool fbits = F4 && a.key_kind != 2;
     uint32_t lt;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
     uint32_t tcount = 0;
@@ -658,10 +752,11 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
         uint32_t am = kNeverPasses;
         if (c < nqt) {
           am = P_am(q0 + c);
-          if (MODE == 1 && a.thr_pos && !dense) {
+          if (BM && a.thr_pos && !dense) {
             const uint32_t td = P_td(q0 + c);
             am = td >= first + kPRows - 1 ? am : td < first ? am + 1 : kExactCompare;
           }
+          if (fbits && am < kNeverPasses) am = __float_as_uint((float)am);  // exact: am <= 2^24
         }
         wam[32 * h2 + lane] = am;
       }
@@ -679,7 +774,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
       const uint64_t doc = pb * 32 + lane;
       const uint64_t u = dt * 256 + rank * kPRows + row;
       const bool valid = pb < n_blocks && doc < a.n;
-      const uint32_t dpop = (MODE == 1 && a.key_kind == 2) ? row_popcount(a, doc, valid) : 0u;
+      const uint32_t dpop = (BM && a.key_kind == 2) ? row_popcount(a, doc, valid) : 0u;
       const uint32_t taddr = tmem + ((lq * 32) << 16) + b * 256 + col0;
       const uint32_t nch = col0 >= nt ? 0u : (col0 + 32 >= nt ? 1u : 2u);  // warp-uniform
       uint32_t wcount = 0;
@@ -698,11 +793,11 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           __syncwarp();
           if (lane == 0) arrive_remote(acc_empty0 + 8 * b);
         }
-        if (MODE == 1 && a.key_kind == 2) {
+        if (BM && a.key_kind == 2) {
 #pragma unroll
-          for (uint32_t j = 0; j < 32; j++) v[j] = ham_y(v[j], dpop);
+          for (uint32_t j = 0; j < 32; j++) v[j] = ham_y(F4 ? f4_int(v[j]) : v[j], dpop);
         }
-        if (dense) {
+        if (!F4 && dense) {
 #pragma unroll
           for (uint32_t j = 0; j < 32; j++) {
             const uint32_t q = cb + j;
@@ -731,12 +826,17 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
               pass = v[j] >= am;
             else if (MODE == 0)
               pass = desc_key(tc_score(v[j], P_bias(q), P_invq(q), a.inv_norm)) <= P_thr(q);
-            else
-              pass = v[j] > P_thr(q) || (v[j] == P_thr(q) && doc <= P_td(q));
+            else {
+              const uint32_t tq = fbits ? __float_as_uint((float)P_thr(q)) : P_thr(q);
+              pass = v[j] > tq || (v[j] == tq && doc <= P_td(q));
+            }
             hm |= (uint32_t)pass << j;
           }
         }
+        // columns past the tile's queries (never written by the MMAs) keep nothing
         if (!valid) hm = 0;
+        const uint32_t ncols = nqt > cb ? nqt - cb : 0u;
+        hm &= ncols >= 32 ? 0xFFFFFFFFu : (1u << ncols) - 1u;
         while (__any_sync(0xFFFFFFFFu, hm != 0)) {
           const bool has = hm != 0;
           const uint32_t j = has ? (uint32_t)(__ffs(hm) - 1) : 0u;
@@ -774,7 +874,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
           if (pos < a.cap) {
             a.f_keys[(q0 + q) * a.cap + pos] = MODE == 0
                 ? desc_key(tc_score(en.x, P_bias(q0 + q), P_invq(q0 + q), a.inv_norm))
-                : bm_key_q(a, P_pop(q0 + q), en.x);
+                : bm_key_q(a, P_pop(q0 + q), fbits ? (uint32_t)__uint_as_float(en.x) : en.x);
             const uint64_t rpb = (dt * 8 + rank * (kPRows / 32) + (rw_ >> 5)) * a.block_stride;
             a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw_ & 31));
           }
@@ -992,6 +1092,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
   pair_body<1, true>(b_map, a, g);
 }
 
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+    bitmap_fp4_pair_kernel(const __grid_constant__ CUtensorMap b_map, const TcArgs a, const PairGrid g) {
+  pair_body<2, true>(b_map, a, g);
+}
+
 __global__ void __launch_bounds__(kPThreads, 1)
     fastscan_persist_kernel(const __grid_constant__ CUtensorMap b_map, const TcArgs a, const PairGrid g) {
   pair_body<0, false>(b_map, a, g);
@@ -1005,8 +1110,8 @@ __global__ void __launch_bounds__(kPThreads, 1)
 // clusters of two that can be resident at once (each CTA takes a whole SM)
 uint32_t resident_pairs(const void* kernel, size_t smem) {
   static std::mutex mu;
-  static int cached[2] = {0, 0};
-  const int slot = kernel == (const void*)fastscan_pair_kernel ? 0 : 1;
+  static int cached[3] = {0, 0, 0};
+  const int slot = kernel == (const void*)fastscan_pair_kernel ? 0 : kernel == (const void*)bitmap_pair_kernel ? 1 : 2;
   std::lock_guard<std::mutex> lk(mu);
   if (!cached[slot]) {
     cudaLaunchConfig_t cfg = {};
@@ -1044,6 +1149,10 @@ TcForm tc_form(int mode) {
 // kept entries one epilogue warp of the persistent one-CTA form may hold per tile
 uint32_t tc_persist_seg_cap() { return PT<false>::kSegCap; }
 
+// The FP4 form of the bitmap filter takes rows the builders keep whole in
+// shared memory.
+uint32_t tc_fp4_max_words() { return kPRowCacheWords; }
+
 template <int MODE>
 void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool pair) {
   if (!a.n || !a.nq) return;
@@ -1067,10 +1176,19 @@ void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool p
     }
     return;
   }
-  const char* what = MODE == 0 ? "FastScan tensor-core scan" : "bitmap tensor-core scan";
+  const char* what = MODE == 0 ? "FastScan tensor-core scan" : MODE == 1 ? "bitmap tensor-core scan"
+                                                                          : "bitmap FP4 tensor-core scan";
   const uint64_t k_bytes = (uint64_t)a.n_kb * kPKBytes;
   if (!a.n_kb || (MODE == 0 && a.n_kb % 4)) throw std::invalid_argument(std::string(what) + ": bad K extent");
-  a.nt = a.nq >= kPMaxN ? kPMaxN : (uint32_t)((a.nq + 15) / 16 * 16);  // a multiple of 16 in [16, 256]
+  if (MODE == 2) {
+    // query tiles of at most kPF4MaxN columns, balanced: a multiple of 16
+    if (!pair || a.keys || a.qpv > kPRowCacheWords || 4ull * a.n_kb < a.qpv)
+      throw std::invalid_argument(std::string(what) + ": needs CTA pairs, a filter and rows of <= 16 words");
+    const uint64_t qt = (a.nq + kPF4MaxN - 1) / kPF4MaxN;
+    a.nt = (uint32_t)(((a.nq + qt - 1) / qt + 15) / 16 * 16);
+  } else {
+    a.nt = a.nq >= kPMaxN ? kPMaxN : (uint32_t)((a.nq + 15) / 16 * 16);  // a multiple of 16 in [16, 256]
+  }
   CUtensorMap map;
   cuuint64_t gdim[2] = {(cuuint64_t)k_bytes, (cuuint64_t)a.nq};
   cuuint64_t gstride[1] = {(cuuint64_t)k_bytes};
@@ -1083,6 +1201,7 @@ void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool p
   if (MODE == 0 && 255ull * a.pairs_pad >= (1ull << 23)) throw std::invalid_argument(std::string(what) + ": dim too large");
   if (MODE == 1 && (64ull * a.qpv >= (1ull << 24) || 2ull * a.n_kb < a.qpv))
     throw std::invalid_argument(std::string(what) + ": row too long");
+  if (MODE == 2 && 64ull * a.qpv >= (1ull << 23)) throw std::invalid_argument(std::string(what) + ": row too long");
   if (!a.keys && a.block_stride != 1) throw std::invalid_argument(std::string(what) + ": filter needs stride 1");
   const uint64_t n_blocks = (a.n + 31) / 32;
   const uint64_t logical_blocks = (n_blocks + a.block_stride - 1) / a.block_stride;
@@ -1095,7 +1214,7 @@ void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool p
   g.q_tiles = (uint32_t)q_tiles;
   const uint64_t total = doc_tiles * q_tiles;
   if (pair) {
-    auto kernel = MODE == 0 ? fastscan_pair_kernel : bitmap_pair_kernel;
+    auto kernel = MODE == 0 ? fastscan_pair_kernel : MODE == 1 ? bitmap_pair_kernel : bitmap_fp4_pair_kernel;
     const size_t smem = sizeof(PSmem<true>) + 1024;
     OVB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     uint64_t clusters = resident_pairs((const void*)kernel, smem);
@@ -1103,7 +1222,7 @@ void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool p
     g.doc_major = doc_tiles >= 2 * clusters ? 1u : 0u;
     if (clusters > total) clusters = total;
     kernel<<<(unsigned)(2 * clusters), kPThreads, smem, stream>>>(map, a, g);
-  } else {
+  } else if constexpr (MODE != 2) {
     auto kernel = MODE == 0 ? fastscan_persist_kernel : bitmap_persist_kernel;
     const size_t smem = sizeof(PSmem<false>) + 1024;
     OVB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1120,5 +1239,6 @@ void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool p
 
 template void launch_tc_pair<0>(TcArgs, const uint8_t*, cudaStream_t, bool);
 template void launch_tc_pair<1>(TcArgs, const uint8_t*, cudaStream_t, bool);
+template void launch_tc_pair<2>(TcArgs, const uint8_t*, cudaStream_t, bool);
 
 }  // namespace ovb

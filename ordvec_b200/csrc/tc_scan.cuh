@@ -148,7 +148,9 @@ __device__ __forceinline__ uint4 load_codes(const uint8_t* p) {
 
 // MODE 0: FastScan (A = one-hot of nibble codes, B = u8 LUTs, score by the
 // FastScan formula).  MODE 1: bitmap AND-overlap (A = doc bits as 0/1 bytes,
-// B = query bits as 0/1 bytes, acc = overlap, key = n_top - overlap).
+// B = query bits as 0/1 bytes, acc = overlap, key = n_top - overlap).  MODE 2:
+// the bitmap filter on FP4 tensor cores (A, B = bits as e2m1 nibbles of 1.0 /
+// 0, f32 acc = overlap), CTA pairs only.
 }  // namespace tcs
 
 // Forms of the tensor-core scans: one CTA per 256-doc tile (scan_fastscan_tc.cu),
@@ -156,6 +158,7 @@ __device__ __forceinline__ uint4 load_codes(const uint8_t* p) {
 enum class TcForm { kTile, kPersist, kPair };
 TcForm tc_form(int mode);  // MODE 0 FastScan, 1 bitmap
 uint32_t tc_persist_seg_cap();
+uint32_t tc_fp4_max_words();  // longest bitmap row (u64 words) of the FP4 form
 // b_rows = the query operand; pair: CTA pairs, else one CTA per SM
 template <int MODE>
 void launch_tc_pair(tcs::TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool pair);

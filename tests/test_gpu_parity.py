@@ -596,7 +596,7 @@ def test_sign_score_all_and_top_m(orc, corpus):
         assert np.array_equal(got[qi], orc.sign_top_m(words, n, dim, queries[qi], 320))
 
 
-_BITMAP_ENV = ("OVB_BITMAP_TC", "OVB_FASTSCAN_FILTER", "OVB_FASTSCAN_SAMPLE_MULT")
+_BITMAP_ENV = ("OVB_BITMAP_TC", "OVB_FASTSCAN_FILTER", "OVB_FASTSCAN_SAMPLE_MULT", "OVB_BITMAP_FP4")
 
 
 def _bitmap_modes(monkeypatch, fn, **env):
@@ -718,6 +718,45 @@ def test_cta_pair_scan_over_query_chunks(monkeypatch, kind):
         base = out[("tile", "0")]
         for key, got in out.items():
             assert np.array_equal(got, base), (n, key)
+
+
+@pytest.mark.parametrize("kind", ["bitmap", "sign", "multibucket"])
+def test_bitmap_fp4_filter_matches_int8(orc, monkeypatch, kind):
+    """The bitmap filter on the FP4 tensor cores (bits as e2m1 1.0, unit block
+    scales, f32 accumulators) keeps exactly the candidates of the int8 scan:
+    query counts giving one to six balanced query tiles of <= 224 columns
+    (1,300 queries: two launches), rows of 1 to 16 words, a corpus with whole
+    doc tiles per CTA pair (A built once per doc tile) and one small enough for
+    the interleaved tile order."""
+    cases = {
+        "bitmap": [(768, 150_000, 1), (768, 150_000, 225), (768, 100_000, 1024), (1024, 9_000, 449), (64, 100_000, 300),
+                   (320, 100_000, 1300)],
+        "sign": [(768, 100_000, 300), (1024, 9_000, 64), (192, 100_000, 700)],
+        "multibucket": [(64, 100_000, 300), (128, 9_000, 250)],
+    }[kind]
+    for dim, n, nq in cases:
+        docs = ob.synth_docs(97, n, dim)
+        queries, _ = ob.synth_queries(97, n, nq, dim)
+        if kind == "bitmap":
+            ix = ob.Bitmap(dim, dim // 4)
+            ix.add(docs)
+            run = lambda: np.array(ix.top_m_candidates_batched(queries, 400))
+        elif kind == "sign":
+            ix = ob.SignBitmap(dim)
+            ix.add(docs)
+            run = lambda: np.array(ix.top_m_candidates_batched(queries, 400))
+        else:
+            ix = ob.MultiBucketBitmap(dim, 2)
+            ix.add(docs)
+            w = np.eye(4, dtype=np.float32).ravel()
+            run = lambda: np.array(ix.top_m_bilinear_batched(queries, w, 400))
+        on = {"OVB_BITMAP_TC": "1", "OVB_FASTSCAN_FILTER": "1", "OVB_TC_FORM": "pair"}
+        f4, i8 = _bitmap_modes(monkeypatch, run, fp4=on, int8=dict(on, OVB_BITMAP_FP4="0"))
+        monkeypatch.delenv("OVB_TC_FORM", raising=False)
+        assert np.array_equal(f4, i8), (dim, n, nq)
+        if kind == "bitmap":
+            words = orc.bitmap_encode(docs, dim, dim // 4)
+            assert np.array_equal(f4[nq - 1], orc.bitmap_top_m(words, n, dim, dim // 4, queries[nq - 1], 400))
 
 
 @pytest.mark.parametrize("dim,n,nq,m", [(1024, 100_000, 64, 320), (384, 70_001, 300, 700), (192, 40_000, 40, 500)])
