@@ -72,6 +72,9 @@ constexpr uint32_t kPRowCacheWords = 16;  // bitmap rows of up to 16 words stay 
 constexpr uint32_t kPKBytes = 128;
 constexpr uint32_t kPTmemCols = 512;
 constexpr uint32_t kPF4MaxN = 224;                  // FP4 form: query columns per tile (scale factors above)
+// FP4 form: default query columns per tile (balanced: 1,024 queries -> 5 tiles
+// of 208; narrower tiles pay the per-tile synchronisation more often)
+constexpr uint32_t kPF4TileN = kPF4MaxN;
 constexpr uint32_t kSfaCol = 224, kSfbCol = 480;    // FP4 form: scale-factor columns of A and B
 constexpr uint32_t kUnitScales = 0x7F7F7F7Fu;       // four ue8m0 bytes of 2^0
 
@@ -225,6 +228,20 @@ __device__ __forceinline__ uint32_t fp4_ones8(uint32_t x) {
   return v << 1;
 }
 
+// v[j] by a 5-level select tree on the bits of j (no local-memory indexing)
+__device__ __forceinline__ uint32_t pick32(const uint32_t (&v)[32], uint32_t j) {
+  uint32_t t16[16], t8[8], t4[4], t2[2];
+#pragma unroll
+  for (uint32_t i = 0; i < 16; i++) t16[i] = (j & 1) ? v[2 * i + 1] : v[2 * i];
+#pragma unroll
+  for (uint32_t i = 0; i < 8; i++) t8[i] = (j & 2) ? t16[2 * i + 1] : t16[2 * i];
+#pragma unroll
+  for (uint32_t i = 0; i < 4; i++) t4[i] = (j & 4) ? t8[2 * i + 1] : t8[2 * i];
+#pragma unroll
+  for (uint32_t i = 0; i < 2; i++) t2[i] = (j & 8) ? t4[2 * i + 1] : t4[2 * i];
+  return (j & 16) ? t2[1] : t2[0];
+}
+
 // The integer value of an f32 accumulator holding an integer in [0, 2^23)
 // (add 2^23: the integer lands in the mantissa bits).
 __device__ __forceinline__ uint32_t f4_int(uint32_t bits) {
@@ -315,6 +332,9 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
   // A resident per doc tile: built once, read by the doc tile's q_tiles
   // consecutive tiles (whole doc tiles per cluster, rows of <= 12 words)
   const bool resA = PAIR && BM && g.doc_major && n_kb <= (uint32_t)kASlots && a.qpv <= kPRowCacheWords;
+  // resident A in two halves when two doc tiles fit: the builders build the
+  // next doc tile's rows while the MMAs read the current one's
+  const bool resA2 = resA && 2 * n_kb <= (uint32_t)kASlots;
 
   if (t == 32) {
     for (int s = 0; s < kASlots; s++) {
@@ -408,14 +428,16 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
       TileCursor tc_;
       for (tc_.start(g, cluster); tc_.valid(g) && ok; tc_.next(g, n_clusters), tcount++) {
         const uint32_t b = tcount % kBufs;
-        const uint32_t pa_res = tc_.di & 1;            // resident A: phase of this doc tile
+        // resident A: this doc tile's slots and their phase
+        const uint32_t a_base = resA2 ? (tc_.di & 1) * n_kb : 0u;
+        const uint32_t pa_res = (resA2 ? tc_.di >> 1 : tc_.di) & 1;
         const bool last_q = tc_.qt + 1 == g.q_tiles;  // resident A: its last reader
         if (tcount >= kBufs && !mbar_wait_issuer(&S.acc_empty[b], (tcount / kBufs - 1) & 1)) ok = false;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + b * 256;
         for (uint32_t kb = 0; kb < n_kb && ok; kb++, it++) {
           const uint32_t sb = rb_s, pb = rb_p;
-          const uint32_t sa = resA ? kb : ra_s;
+          const uint32_t sa = resA ? a_base + kb : ra_s;
           const uint32_t pa = resA ? pa_res : ra_p;
           // resident A: after the doc tile's first query tile its slots are known
           // full (nothing refills them before its last query tile frees them)
@@ -425,7 +447,9 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
             ok = false;
             break;
           }
-          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          // (operands arrive by TMA, or by builder stores behind a proxy fence and
+          // the barrier: no tcgen05 fence is needed before reading them)
+          if (!PAIR) asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t a0 = smem_u32(S.a[sa]), b0 = smem_u32(S.b[sb]);
           const bool free_a = !resA || last_q;
           if (PAIR) {
@@ -546,7 +570,10 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
             }
           }
           if (resA && qt_ != 0) continue;  // the doc tile's A is resident: built at its first query tile
-          const uint64_t dc = tc_.di;  // resident A: doc tiles this cluster started before
+          // resident A: earlier uses of this doc tile's slots (doc tiles this
+          // cluster started before, or of the same parity with two halves)
+          const uint64_t dc = resA2 ? tc_.di >> 1 : tc_.di;
+          const uint32_t s_base = resA2 ? (tc_.di & 1) * n_kb : 0u;
           const uint32_t base0 = a_row[0], rr = r & 7;
           constexpr uint32_t kWordsPerKb = F4 ? 4 : 2;  // 128 bytes: 256 nibbles or 128 bytes of 0/1
 #pragma unroll
@@ -554,10 +581,14 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
             if (kb >= n_kb) break;
             uint32_t s;
             if (resA) {
-              s = kb;
-              if (dc > 0) {  // the previous doc tile's last query tile has read this slot
+              s = s_base + kb;
+              if (dc > 0) {  // the slot's previous doc tile has been read by its last query tile
+                // (with two halves the builders run a doc tile ahead: they sleep
+                // rather than poll, leaving the issue slots to the epilogue and MMA warps)
                 bool w = true;
-                if (lane == 0) w = !aborted(S) && mbar_wait_issuer(&S.empty_a[s], (uint32_t)((dc - 1) & 1));
+                if (lane == 0)
+                  w = !aborted(S) && (resA2 ? mbar_wait(&S.empty_a[s], (uint32_t)((dc - 1) & 1))
+                                            : mbar_wait_issuer(&S.empty_a[s], (uint32_t)((dc - 1) & 1)));
                 w = __shfl_sync(0xFFFFFFFFu, w, 0);
                 if (!w && lane == 0 && !aborted(S)) raise_abort(S, a.err);
                 __syncwarp();
@@ -692,7 +723,10 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
     const uint32_t e = (uint32_t)warp - 2 - kPBuildWarps;  // 0..15
     const uint32_t et = (uint32_t)t - 32 * (2 + kPBuildWarps);
     const uint32_t lq = (uint32_t)warp & 3;  // TMEM lane quarter (hardware rule: warp % 4)
-    const uint32_t col0 = (e >> 2) * 64;     // this warp's 64 accumulator columns
+    // this warp's accumulator columns: 64, or 32 for FP4 tiles of <= 128 queries
+    // (one 32-column load a warp: the accumulator is released after one read)
+    const uint32_t wcols = (F4 && nt <= 128) ? 32u : 64u;
+    const uint32_t col0 = (e >> 2) * wcols;
     const uint32_t row = lq * 32 + lane;
     const uint32_t acc_empty0 = peer_addr(smem_u32(&S.acc_empty[0]), 0);
     // S.qp: [amin | tdoc (bitmap) or bias (FastScan) | thr | qpop (bitmap) or invq (FastScan)] x kPMaxQ
@@ -729,157 +763,275 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& b_map, const TcArgs
       }
     }
     epi_sync();
-    uint32_t* wam = S.wamin[e];
     uint2* list = S.list[e];
-    // FP4 form: accumulators are f32 bits (compared as bits) except for sign
-    // bitmaps, whose epilogue transform needs the integer
-    const bool fbits = F4 && a.key_kind != 2;
     uint32_t lt;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
-    uint32_t tcount = 0;
-    TileCursor tc_;
-    for (tc_.start(g, cluster); tc_.valid(g); tc_.next(g, n_clusters), tcount++) {
-      const uint64_t dt = tc_.dt;
-      const uint32_t qt_ = tc_.qt;
-      const uint64_t q0 = (uint64_t)qt_ * nt;
-      const uint32_t nqt = (uint32_t)((a.nq - q0) < nt ? (a.nq - q0) : nt);
-      const uint32_t b = tcount % kBufs;
-      const uint64_t first = dt * 256 + rank * kPRows;
-      // thresholds of this warp's columns for this tile
-#pragma unroll
-      for (uint32_t h2 = 0; h2 < 2; h2++) {
-        const uint32_t c = col0 + 32 * h2 + lane;
-        uint32_t am = kNeverPasses;
-        if (c < nqt) {
-          am = P_am(q0 + c);
-          if (BM && a.thr_pos && !dense) {
-            const uint32_t td = P_td(q0 + c);
-            am = td >= first + kPRows - 1 ? am : td < first ? am + 1 : kExactCompare;
-          }
-          if (fbits && am < kNeverPasses) am = __float_as_uint((float)am);  // exact: am <= 2^24
-        }
-        wam[32 * h2 + lane] = am;
-      }
-      const bool any_exact = __any_sync(0xFFFFFFFFu, wam[lane] == kExactCompare || wam[32 + lane] == kExactCompare);
+    const uint32_t nch = col0 >= nt ? 0u : (col0 + 32 >= nt || wcols == 32 ? 1u : 2u);  // 32-column chunks (warp-uniform)
+    // A tile's kept entries -> the candidate rows: a slot per entry by a global
+    // atomic on its query's count; a list that overflowed fails every query of
+    // the warp's columns (bit 31 > cap).
+    auto flush = [&](uint32_t wcount, uint64_t q0, uint64_t dt, uint32_t nqt) {
       __syncwarp();
-      bool ready = false;
-      if (lane == 0) ready = !aborted(S) && mbar_wait_cluster(&S.acc_full[b], (tcount / kBufs) & 1);
-      ready = __shfl_sync(0xFFFFFFFFu, ready, 0);
-      if (!ready) {
-        if (lane == 0 && !aborted(S)) raise_abort(S, a.err);
-        break;
+      if (wcount > kPSegCap) {
+        for (uint32_t j = lane; j < wcols; j += 32)
+          if (col0 + j < nqt) atomicOr(&a.cnt[q0 + col0 + j], 0x80000000u);
       }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint64_t pb = (dt * 8 + rank * (kPRows / 32) + (row >> 5)) * a.block_stride;
-      const uint64_t doc = pb * 32 + lane;
-      const uint64_t u = dt * 256 + rank * kPRows + row;
-      const bool valid = pb < n_blocks && doc < a.n;
-      const uint32_t dpop = (BM && a.key_kind == 2) ? row_popcount(a, doc, valid) : 0u;
-      const uint32_t taddr = tmem + ((lq * 32) << 16) + b * 256 + col0;
-      const uint32_t nch = col0 >= nt ? 0u : (col0 + 32 >= nt ? 1u : 2u);  // warp-uniform
-      uint32_t wcount = 0;
-      if (nch == 0) {  // nothing to read: release the accumulator at once
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) arrive_remote(acc_empty0 + 8 * b);
+      const uint32_t tot = wcount < kPSegCap ? wcount : kPSegCap;
+      for (uint32_t j = lane; j < tot; j += 32) {
+        const uint2 en = list[j];
+        const uint32_t q = en.y & 0xFFFFu, rw_ = en.y >> 16;
+        const uint32_t pos = atomicAdd(&a.cnt[q0 + q], 1u);
+        if (pos < a.cap) {
+          a.f_keys[(q0 + q) * a.cap + pos] = MODE == 0
+              ? desc_key(tc_score(en.x, P_bias(q0 + q), P_invq(q0 + q), a.inv_norm))
+              : bm_key_q(a, P_pop(q0 + q), en.x);
+          const uint64_t rpb = (dt * 8 + rank * (kPRows / 32) + (rw_ >> 5)) * a.block_stride;
+          a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw_ & 31));
+        }
       }
-      for (uint32_t c = 0; c < nch; c++) {
-        const uint32_t cb = col0 + 32 * c;
-        uint32_t v[32];
+      __syncwarp();  // the list is reused by the next tile
+    };
+    if constexpr (F4) {
+      // FP4 form: the f32 sums of constant-weight and multi-bucket keys are
+      // compared as bits with the f32 bits of each column's integer threshold
+      // (non-negative floats order like their bit patterns); sign bitmaps take
+      // the integer sums.  Both 32-column chunks are read back to back (one
+      // tensor-memory latency) and the buffer released before any compare; the
+      // slots of a tile's kept entries are reserved by atomics whose results are
+      // first used during the next tile.
+      uint32_t* wam = S.wamin[e];
+      const bool fbits = a.key_kind != 2;
+      // this lane's entry of the previous tile, its slot reserved
+      bool pend = false;
+      uint32_t p_pos = 0, p_key = 0, p_id = 0;
+      uint64_t p_q = 0;
+      auto finish = [&]() {
+        if (pend && p_pos < a.cap) {
+          a.f_keys[p_q * a.cap + p_pos] = p_key;
+          a.f_ids[p_q * a.cap + p_pos] = p_id;
+        }
+        pend = false;
+      };
+      uint32_t tcount = 0;
+      TileCursor tc_;
+      for (tc_.start(g, cluster); tc_.valid(g); tc_.next(g, n_clusters), tcount++) {
+        const uint64_t dt = tc_.dt;
+        const uint64_t q0 = (uint64_t)tc_.qt * nt;
+        const uint32_t nqt = (uint32_t)((a.nq - q0) < nt ? (a.nq - q0) : nt);
+        const uint32_t b = tcount % kBufs;
+        const uint64_t first = dt * 256 + rank * kPRows;
+        // thresholds of this warp's columns for this tile
+#pragma unroll
+        for (uint32_t h2 = 0; h2 < 2; h2++) {
+          const uint32_t c = col0 + 32 * h2 + lane;
+          uint32_t am = kNeverPasses;
+          if (c < nqt) {
+            am = P_am(q0 + c);
+            if (a.thr_pos) {
+              const uint32_t td = P_td(q0 + c);
+              am = td >= first + kPRows - 1 ? am : td < first ? am + 1 : kExactCompare;
+            }
+            if (fbits && am < kNeverPasses) am = __float_as_uint((float)am);  // exact: am <= 2^24
+          }
+          wam[32 * h2 + lane] = am;
+        }
+        const bool any_exact = __any_sync(0xFFFFFFFFu, wam[lane] == kExactCompare || wam[32 + lane] == kExactCompare);
         __syncwarp();
-        tmem_ld32(taddr + 32 * c, v);
-        if (c + 1 == nch) {  // the last chunk is in registers: release the accumulator to the MMA
+        bool ready = false;
+        if (lane == 0) ready = !aborted(S) && mbar_wait_cluster(&S.acc_full[b], (tcount / kBufs) & 1);
+        ready = __shfl_sync(0xFFFFFFFFu, ready, 0);
+        if (!ready) {
+          if (lane == 0 && !aborted(S)) raise_abort(S, a.err);
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint64_t doc = first + row;  // filter: block stride 1
+        const bool valid = doc < a.n;
+        const uint32_t taddr = tmem + ((lq * 32) << 16) + b * 256 + col0;
+        const uint32_t dpop = fbits ? 0u : row_popcount(a, doc, valid);
+        uint32_t wcount = 0;
+        if (nch == 0) {  // nothing to read: release the accumulator at once
           asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
           __syncwarp();
           if (lane == 0) arrive_remote(acc_empty0 + 8 * b);
         }
-        if (BM && a.key_kind == 2) {
-#pragma unroll
-          for (uint32_t j = 0; j < 32; j++) v[j] = ham_y(F4 ? f4_int(v[j]) : v[j], dpop);
-        }
-        if (!F4 && dense) {
-#pragma unroll
-          for (uint32_t j = 0; j < 32; j++) {
-            const uint32_t q = cb + j;
-            if (valid && q < nqt)
-              a.keys[(q0 + q) * a.ld + u] = MODE == 0
-                  ? desc_key(tc_score(v[j], P_bias(q0 + q), P_invq(q0 + q), a.inv_norm))
-                  : bm_key_q(a, P_pop(q0 + q), v[j]);
+        for (uint32_t c = 0; c < nch; c++) {
+          const uint32_t cb = col0 + 32 * c;
+          uint32_t v[32];
+          __syncwarp();
+          tmem_ld32(taddr + 32 * c, v);
+          if (c + 1 == nch) {  // the last chunk is in registers: release the accumulator to the MMAs
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) arrive_remote(acc_empty0 + 8 * b);
           }
-          continue;
-        }
-        uint32_t hm = 0;  // the columns (queries) this lane's doc passes
-        if (!any_exact) {
+          if (c == 0) finish();  // the previous tile's slots have long been reserved
+          if (!fbits) {
 #pragma unroll
-          for (uint32_t j = 0; j < 32; j += 4) {
-            const uint4 am = *reinterpret_cast<const uint4*>(&wam[32 * c + j]);
-            hm |= ((uint32_t)(v[j] >= am.x) << j) | ((uint32_t)(v[j + 1] >= am.y) << (j + 1)) |
-                  ((uint32_t)(v[j + 2] >= am.z) << (j + 2)) | ((uint32_t)(v[j + 3] >= am.w) << (j + 3));
+            for (uint32_t j = 0; j < 32; j++) v[j] = ham_y(f4_int(v[j]), dpop);
           }
-        } else {
+          uint32_t hm = 0;  // the columns (queries) this lane's doc passes
+          if (!any_exact) {
 #pragma unroll
-          for (uint32_t j = 0; j < 32; j++) {
-            const uint32_t q = q0 + cb + j;
-            const uint32_t am = wam[32 * c + j];
-            bool pass;
-            if (am != kExactCompare)
-              pass = v[j] >= am;
-            else if (MODE == 0)
-              pass = desc_key(tc_score(v[j], P_bias(q), P_invq(q), a.inv_norm)) <= P_thr(q);
-            else {
-              const uint32_t tq = fbits ? __float_as_uint((float)P_thr(q)) : P_thr(q);
-              pass = v[j] > tq || (v[j] == tq && doc <= P_td(q));
+            for (uint32_t j = 0; j < 32; j += 4) {
+              const uint4 am = *reinterpret_cast<const uint4*>(&wam[32 * c + j]);
+              hm |= ((uint32_t)(v[j] >= am.x) << j) | ((uint32_t)(v[j + 1] >= am.y) << (j + 1)) |
+                    ((uint32_t)(v[j + 2] >= am.z) << (j + 2)) | ((uint32_t)(v[j + 3] >= am.w) << (j + 3));
             }
-            hm |= (uint32_t)pass << j;
+          } else {
+#pragma unroll
+            for (uint32_t j = 0; j < 32; j++) {
+              const uint32_t q = (uint32_t)q0 + cb + j;
+              const uint32_t am = wam[32 * c + j];
+              const uint32_t tq = fbits ? __float_as_uint((float)P_thr(q)) : P_thr(q);
+              const bool pass = am != kExactCompare ? v[j] >= am : v[j] > tq || (v[j] == tq && doc <= P_td(q));
+              hm |= (uint32_t)pass << j;
+            }
+          }
+          // columns past the tile's queries (never written by the MMAs) keep nothing
+          if (!valid) hm = 0;
+          const uint32_t ncols = nqt > cb ? nqt - cb : 0u;
+          hm &= ncols >= 32 ? 0xFFFFFFFFu : (1u << ncols) - 1u;
+          while (__any_sync(0xFFFFFFFFu, hm != 0)) {
+            const bool has = hm != 0;
+            const uint32_t j = has ? (uint32_t)(__ffs(hm) - 1) : 0u;
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+            const uint32_t pos = wcount + __popc(bal & lt);
+            if (has && pos < kPSegCap) {
+              const uint32_t x = pick32(v, j);
+              list[pos] = make_uint2(fbits ? (uint32_t)__uint_as_float(x) : x, (cb + j) | (row << 16));
+            }
+            wcount += __popc(bal);
+            hm &= hm - 1;
           }
         }
-        // columns past the tile's queries (never written by the MMAs) keep nothing
-        if (!valid) hm = 0;
-        const uint32_t ncols = nqt > cb ? nqt - cb : 0u;
-        hm &= ncols >= 32 ? 0xFFFFFFFFu : (1u << ncols) - 1u;
-        while (__any_sync(0xFFFFFFFFu, hm != 0)) {
-          const bool has = hm != 0;
-          const uint32_t j = has ? (uint32_t)(__ffs(hm) - 1) : 0u;
-          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
-          const uint32_t pos = wcount + __popc(bal & lt);
-          if (has && pos < kPSegCap) {
-            // v[j] by a 5-level select tree on the bits of j
-            uint32_t t16[16], t8[8], t4[4], t2[2];
-#pragma unroll
-            for (uint32_t i = 0; i < 16; i++) t16[i] = (j & 1) ? v[2 * i + 1] : v[2 * i];
-#pragma unroll
-            for (uint32_t i = 0; i < 8; i++) t8[i] = (j & 2) ? t16[2 * i + 1] : t16[2 * i];
-#pragma unroll
-            for (uint32_t i = 0; i < 4; i++) t4[i] = (j & 4) ? t8[2 * i + 1] : t8[2 * i];
-#pragma unroll
-            for (uint32_t i = 0; i < 2; i++) t2[i] = (j & 8) ? t4[2 * i + 1] : t4[2 * i];
-            const uint32_t acc = (j & 16) ? t2[1] : t2[0];
-            list[pos] = make_uint2(acc, (cb + j) | (row << 16));
-          }
-          wcount += __popc(bal);
-          hm &= hm - 1;
-        }
-      }
-      if (!dense) {
+        if (nch == 0) finish();
         __syncwarp();
-        if (wcount > kPSegCap) {  // entries were lost: fail every query of this warp's columns (bit 31 > cap)
-          for (uint32_t j = lane; j < 64; j += 32)
-            if (col0 + j < nqt) atomicOr(&a.cnt[q0 + col0 + j], 0x80000000u);
-        }
-        const uint32_t tot = wcount < kPSegCap ? wcount : kPSegCap;
-        for (uint32_t j = lane; j < tot; j += 32) {
-          const uint2 en = list[j];
+        if (wcount > 32) {
+          flush(wcount, q0, dt, nqt);  // more than one entry per lane (or lost ones): reserve and write now
+        } else if (lane < wcount) {
+          // reserve this lane's slot now, write the entry during the next tile
+          const uint2 en = list[lane];
           const uint32_t q = en.y & 0xFFFFu, rw_ = en.y >> 16;
-          const uint32_t pos = atomicAdd(&a.cnt[q0 + q], 1u);
-          if (pos < a.cap) {
-            a.f_keys[(q0 + q) * a.cap + pos] = MODE == 0
-                ? desc_key(tc_score(en.x, P_bias(q0 + q), P_invq(q0 + q), a.inv_norm))
-                : bm_key_q(a, P_pop(q0 + q), fbits ? (uint32_t)__uint_as_float(en.x) : en.x);
-            const uint64_t rpb = (dt * 8 + rank * (kPRows / 32) + (rw_ >> 5)) * a.block_stride;
-            a.f_ids[(q0 + q) * a.cap + pos] = (uint32_t)(rpb * 32 + (rw_ & 31));
-          }
+          p_q = q0 + q;
+          p_pos = atomicAdd(&a.cnt[p_q], 1u);
+          p_key = bm_key_q(a, P_pop(p_q), en.x);
+          p_id = (uint32_t)(first + rw_);
+          pend = true;
         }
         __syncwarp();  // the list is reused by the next tile
+      }
+      finish();
+    } else {
+      uint32_t* wam = S.wamin[e];
+      uint32_t tcount = 0;
+      TileCursor tc_;
+      for (tc_.start(g, cluster); tc_.valid(g); tc_.next(g, n_clusters), tcount++) {
+        const uint64_t dt = tc_.dt;
+        const uint32_t qt_ = tc_.qt;
+        const uint64_t q0 = (uint64_t)qt_ * nt;
+        const uint32_t nqt = (uint32_t)((a.nq - q0) < nt ? (a.nq - q0) : nt);
+        const uint32_t b = tcount % kBufs;
+        const uint64_t first = dt * 256 + rank * kPRows;
+        // thresholds of this warp's columns for this tile
+#pragma unroll
+        for (uint32_t h2 = 0; h2 < 2; h2++) {
+          const uint32_t c = col0 + 32 * h2 + lane;
+          uint32_t am = kNeverPasses;
+          if (c < nqt) {
+            am = P_am(q0 + c);
+            if (BM && a.thr_pos && !dense) {
+              const uint32_t td = P_td(q0 + c);
+              am = td >= first + kPRows - 1 ? am : td < first ? am + 1 : kExactCompare;
+            }
+          }
+          wam[32 * h2 + lane] = am;
+        }
+        const bool any_exact = __any_sync(0xFFFFFFFFu, wam[lane] == kExactCompare || wam[32 + lane] == kExactCompare);
+        __syncwarp();
+        bool ready = false;
+        if (lane == 0) ready = !aborted(S) && mbar_wait_cluster(&S.acc_full[b], (tcount / kBufs) & 1);
+        ready = __shfl_sync(0xFFFFFFFFu, ready, 0);
+        if (!ready) {
+          if (lane == 0 && !aborted(S)) raise_abort(S, a.err);
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint64_t pb = (dt * 8 + rank * (kPRows / 32) + (row >> 5)) * a.block_stride;
+        const uint64_t doc = pb * 32 + lane;
+        const uint64_t u = dt * 256 + rank * kPRows + row;
+        const bool valid = pb < n_blocks && doc < a.n;
+        const uint32_t dpop = (BM && a.key_kind == 2) ? row_popcount(a, doc, valid) : 0u;
+        const uint32_t taddr = tmem + ((lq * 32) << 16) + b * 256 + col0;
+        uint32_t wcount = 0;
+        if (nch == 0) {  // nothing to read: release the accumulator at once
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) arrive_remote(acc_empty0 + 8 * b);
+        }
+        for (uint32_t c = 0; c < nch; c++) {
+          const uint32_t cb = col0 + 32 * c;
+          uint32_t v[32];
+          __syncwarp();
+          tmem_ld32(taddr + 32 * c, v);
+          if (c + 1 == nch) {  // the last chunk is in registers: release the accumulator to the MMA
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) arrive_remote(acc_empty0 + 8 * b);
+          }
+          if (BM && a.key_kind == 2) {
+#pragma unroll
+            for (uint32_t j = 0; j < 32; j++) v[j] = ham_y(v[j], dpop);
+          }
+          if (dense) {
+#pragma unroll
+            for (uint32_t j = 0; j < 32; j++) {
+              const uint32_t q = cb + j;
+              if (valid && q < nqt)
+                a.keys[(q0 + q) * a.ld + u] = MODE == 0
+                    ? desc_key(tc_score(v[j], P_bias(q0 + q), P_invq(q0 + q), a.inv_norm))
+                    : bm_key_q(a, P_pop(q0 + q), v[j]);
+            }
+            continue;
+          }
+          uint32_t hm = 0;  // the columns (queries) this lane's doc passes
+          if (!any_exact) {
+#pragma unroll
+            for (uint32_t j = 0; j < 32; j += 4) {
+              const uint4 am = *reinterpret_cast<const uint4*>(&wam[32 * c + j]);
+              hm |= ((uint32_t)(v[j] >= am.x) << j) | ((uint32_t)(v[j + 1] >= am.y) << (j + 1)) |
+                    ((uint32_t)(v[j + 2] >= am.z) << (j + 2)) | ((uint32_t)(v[j + 3] >= am.w) << (j + 3));
+            }
+          } else {
+#pragma unroll
+            for (uint32_t j = 0; j < 32; j++) {
+              const uint32_t q = q0 + cb + j;
+              const uint32_t am = wam[32 * c + j];
+              bool pass;
+              if (am != kExactCompare)
+                pass = v[j] >= am;
+              else if (MODE == 0)
+                pass = desc_key(tc_score(v[j], P_bias(q), P_invq(q), a.inv_norm)) <= P_thr(q);
+              else
+                pass = v[j] > P_thr(q) || (v[j] == P_thr(q) && doc <= P_td(q));
+              hm |= (uint32_t)pass << j;
+            }
+          }
+          // columns past the tile's queries (never written by the MMAs) keep nothing
+          if (!valid) hm = 0;
+          const uint32_t ncols = nqt > cb ? nqt - cb : 0u;
+          hm &= ncols >= 32 ? 0xFFFFFFFFu : (1u << ncols) - 1u;
+          while (__any_sync(0xFFFFFFFFu, hm != 0)) {
+            const bool has = hm != 0;
+            const uint32_t j = has ? (uint32_t)(__ffs(hm) - 1) : 0u;
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+            const uint32_t pos = wcount + __popc(bal & lt);
+            if (has && pos < kPSegCap) list[pos] = make_uint2(pick32(v, j), (cb + j) | (row << 16));
+            wcount += __popc(bal);
+            hm &= hm - 1;
+          }
+        }
+        if (!dense) flush(wcount, q0, dt, nqt);
       }
     }
 #undef P_am
@@ -1181,10 +1333,15 @@ void launch_tc_pair(TcArgs a, const uint8_t* b_rows, cudaStream_t stream, bool p
   const uint64_t k_bytes = (uint64_t)a.n_kb * kPKBytes;
   if (!a.n_kb || (MODE == 0 && a.n_kb % 4)) throw std::invalid_argument(std::string(what) + ": bad K extent");
   if (MODE == 2) {
-    // query tiles of at most kPF4MaxN columns, balanced: a multiple of 16
+    // query tiles of at most kPF4TileN columns (OVB_FP4_TILE_N: 16..224), balanced: a multiple of 16
     if (!pair || a.keys || a.qpv > kPRowCacheWords || 4ull * a.n_kb < a.qpv)
       throw std::invalid_argument(std::string(what) + ": needs CTA pairs, a filter and rows of <= 16 words");
-    const uint64_t qt = (a.nq + kPF4MaxN - 1) / kPF4MaxN;
+    uint32_t tile_n = kPF4TileN;
+    if (const char* e = getenv("OVB_FP4_TILE_N")) {
+      const long v = strtol(e, nullptr, 10);
+      if (v >= 16 && v <= (long)kPF4MaxN) tile_n = (uint32_t)(v / 16 * 16);
+    }
+    const uint64_t qt = (a.nq + tile_n - 1) / tile_n;
     a.nt = (uint32_t)(((a.nq + qt - 1) / qt + 15) / 16 * 16);
   } else {
     a.nt = a.nq >= kPMaxN ? kPMaxN : (uint32_t)((a.nq + 15) / 16 * 16);  // a multiple of 16 in [16, 256]
