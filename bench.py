@@ -1034,24 +1034,31 @@ def main():
     hbm_peak, bf16_peak, peak_kind = measured_peaks()
     code_bytes = N_DOCS * QPV * 8
 
+    fp4 = os.environ.get("OVB_BITMAP_FP4", "1") != "0"
+
     def roof_batched(ms):
-        """bitmap_pair_kernel: the overlap popcount(q AND d) of every (doc,
-        query) pair as an exact u8 GEMM on tcgen05 (kind::i8), A = each doc's
-        768 bits as 0/1 bytes (built in shared memory), B = the queries' bits
-        as 0/1 bytes.  Algorithmic ops = 2 * docs * queries * 768; peak = 2 x
-        the measured dense bf16 rate (kind::i8 issues twice the MACs of
-        kind::f16)."""
+        """The filter scan: the overlap popcount(q AND d) of every (doc, query)
+        pair as an exact tensor-core GEMM on 0/1 operands.  Default form
+        bitmap_fp4_pair_kernel (kind::mxf4: bits as e2m1 1.0 / 0 with unit
+        block scales, f32 sums; peak = 4 x the measured dense bf16 rate, the
+        ratio of the nominal dense FP4 and bf16 rates); with OVB_BITMAP_FP4=0
+        bitmap_pair_kernel (kind::i8 on 0/1 bytes; peak = 2 x measured bf16).
+        Algorithmic ops = 2 * docs * queries * 768 either way."""
         ops = 2 * N_DOCS * NQ * QPV * 64
         achieved = ops / (ms * 1e-3) / 1e12
-        return {"bound": "tensor", "achieved": achieved, "peak": 2 * bf16_peak, "unit": "TOPS (int8)",
-                "frac": achieved / (2 * bf16_peak), "traffic": PAIR_FILTER_DRAM_BYTES,
+        peak = (4 if fp4 else 2) * bf16_peak
+        return {"bound": "tensor", "achieved": achieved, "peak": peak,
+                "unit": "TOPS (0/1 operands; FP4 e2m1 MMAs)" if fp4 else "TOPS (int8)",
+                "frac": achieved / peak, "frac_of_int8_peak": achieved / (2 * bf16_peak),
+                "traffic": PAIR_FILTER_DRAM_BYTES,
                 "traffic_unit": "DRAM bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                 "algorithmic_hbm_bytes_per_launch": code_bytes + NQ * QPV * 64,
                 "codes_gbs": code_bytes / (ms * 1e-3) / 1e9,
-                "kernel": "bitmap_pair_kernel (filter epilogue)", "queries_per_launch": NQ,
+                "kernel": ("bitmap_fp4_pair_kernel" if fp4 else "bitmap_pair_kernel") + " (filter epilogue)",
+                "queries_per_launch": NQ,
                 "algorithmic_ops_per_launch": ops, "launch_ms": ms, "launches_timed": len(stage_rows),
                 "timing": "mean of the scan-stage CUDA events of every timed step (launching stream)",
-                "peak_source": f"2 x {peak_kind} bf16 dense TFLOP/s (burst)"}
+                "peak_source": f"{4 if fp4 else 2} x {peak_kind} bf16 dense TFLOP/s (burst)"}
 
     def roof_plain(ms):
         """One query: popc_rows_kernel (CUDA cores), bound by HBM: the codes
@@ -1068,7 +1075,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u8-bits/s32-acc + f64 rerank", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": ("e2m1-bits/f32-acc" if fp4 else "u8-bits/s32-acc") + " + f64 rerank", "data": "synthetic",
         "config": headline_config(world),
         "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": NQ * DIM * 4,
                 "d2h_bytes_per_step": NQ * K * (4 + 8), "ms_per_step": e2e_total / e2e_steps, "steps": e2e_steps,
