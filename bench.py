@@ -54,9 +54,10 @@ BUILD_CHUNK = 1_000_000
 STAGES = ["prep", "threshold", "scan", "select", "rerank", "final_select"]
 WORKLOAD = (f"large_corpus_bitmap_two_stage: Bitmap n_top={N_TOP} top-{M} -> RankQuant b={BITS} asymmetric "
             f"rerank top-{K}; N={N_DOCS} dim={DIM}; {NQ} queries per step")
-# DRAM traffic of one filter launch of bitmap_pair_kernel at this workload (ncu
-# dram__bytes_read.sum + dram__bytes_write.sum): the codes cross HBM about once.
-PAIR_FILTER_DRAM_BYTES = None
+# DRAM traffic of one filter launch of bitmap_fp4_pair_kernel at this workload
+# (ncu dram__bytes_read.sum 961,795,328 + dram__bytes_write.sum 65,410,304 on the
+# full 10M-doc launch): the codes cross HBM once, the rest is the kept candidates.
+PAIR_FILTER_DRAM_BYTES = 1_027_205_632
 # FastScan two-stage configuration (extra key)
 FS_N, FS_DIM, FS_NQ, FS_K, FS_M, FS_SEED = 171_332, 1024, 1000, 10, 1000, 0x0DD5EED2
 # DRAM traffic of one filter launch of fastscan_persist_kernel at that workload, from an ncu capture
