@@ -1119,12 +1119,21 @@ def main():
         line["identical_top100_vs_cpu"] = same
     if extras:
         del mb, multibucket
-        line["fastscan_two_stage"] = fastscan_run(ob, torch, dev, args, cpu)
-        line["mixed_batch"] = mixed_run(ob, mixed_q, args.steps) if mixed_q > 0 else None
-        line["sign_b1_plain"] = sign_plain_run(ob, torch, dev, args.plain_queries, cpu)
-        line["serving_multi"] = serving_multi_run(ob, args.serve_seconds, [20_000.0, 100_000.0, args.serve_rate]) \
-            if args.serve_seconds > 0 else None
-        line["rank_modes"] = rank_modes_run(ob, torch, dev, args.plain_queries)
+
+        def extra(name, fn):
+            """One optional side workload: an error in it is recorded in the line
+            (the headline above stands on its own)."""
+            try:
+                line[name] = fn()
+            except Exception as exc:  # noqa: BLE001 -- reported, not hidden
+                line[name] = {"error": f"{type(exc).__name__}: {exc}"}
+
+        extra("fastscan_two_stage", lambda: fastscan_run(ob, torch, dev, args, cpu))
+        extra("mixed_batch", lambda: mixed_run(ob, mixed_q, args.steps) if mixed_q > 0 else None)
+        extra("sign_b1_plain", lambda: sign_plain_run(ob, torch, dev, args.plain_queries, cpu))
+        extra("serving_multi", lambda: serving_multi_run(ob, args.serve_seconds, [20_000.0, 100_000.0, args.serve_rate])
+              if args.serve_seconds > 0 else None)
+        extra("rank_modes", lambda: rank_modes_run(ob, torch, dev, args.plain_queries))
     group.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -154,7 +154,7 @@ void launch_encode(int kind, const float* vecs, uint64_t n, uint32_t dim, uint32
   while (len < dim) len <<= 1;
   const size_t smem = (size_t)len * 8 + (size_t)dim * 2;
   if (smem > 227 * 1024) throw std::invalid_argument("dim too large for the device rank transform");
-  OVB_CUDA(cudaFuncSetAttribute(rank_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(rank_encode_kernel);
   const unsigned threads = len >= 1024 ? 512 : 256;
   for (uint64_t d0 = 0; d0 < n; d0 += 0x7FFFFFFF) {
     uint64_t cnt = n - d0 < 0x7FFFFFFF ? n - d0 : 0x7FFFFFFF;

@@ -13,8 +13,11 @@
 #include <stdint.h>
 
 #include <cstring>
+#include <mutex>
+#include <set>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 namespace ovb {
 
@@ -29,11 +32,37 @@ struct CudaError : std::runtime_error {
   explicit CudaError(const std::string& s) : std::runtime_error(s) {}
 };
 
-// Kernel launches issued by this thread (benchmark instrumentation).
+// Lets `kernel` take as much dynamic shared memory as the current device allows
+// beside its static shared memory, once per (kernel, device).  A launch needs
+// the opt-in once static + dynamic exceed 48 KiB; setting the limit to the
+// launch's own size instead would let two host threads with different sizes
+// lower it under each other's launches.
+template <class K>
+void allow_dynamic_smem(K* kernel) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  OVB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({(const void*)kernel, dev})) return;
+  int optin = 0;
+  OVB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  OVB_CUDA(cudaFuncGetAttributes(&fa, (const void*)kernel));
+  OVB_CUDA(cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - (int)fa.sharedSizeBytes));
+  done.insert({(const void*)kernel, dev});
+}
+
+// Kernel launches issued by this thread (benchmark instrumentation).  A launch
+// error names the launching function and line.
 extern thread_local uint64_t tl_launch_counter;
-inline void launched() {
+inline void launched(const char* fn = __builtin_FUNCTION(), int line = __builtin_LINE()) {
   tl_launch_counter++;
-  OVB_CUDA(cudaGetLastError());
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw CudaError(std::string("kernel launch in ") + fn + " (line " + std::to_string(line) + "): " +
+                    cudaGetErrorString(e));
 }
 
 // f32::total_cmp ascending maps to unsigned ascending of

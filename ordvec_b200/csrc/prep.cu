@@ -247,8 +247,7 @@ void launch_bitmap_query(const float* q, uint64_t nq, uint32_t dim, uint32_t n_t
   while (len < dim) len <<= 1;
   size_t smem = (size_t)len * 8;
   if (smem > 227 * 1024) throw std::invalid_argument("Bitmap query dim too large for the device path (dim <= 16384)");
-  if (smem > 48 * 1024)
-    OVB_CUDA(cudaFuncSetAttribute(bitmap_query_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(bitmap_query_kernel);
   bitmap_query_kernel<<<(unsigned)nq, 512, smem, stream>>>(q, dim, n_top, len, out);
   launched();
 }

@@ -343,7 +343,7 @@ void launch_rerank_tc(const uint8_t* codes, uint64_t n, uint32_t dim, uint32_t b
   const size_t smem = sizeof(RrSmem) + 1024;
 #define OVB_RR(B)                                                                                                \
   do {                                                                                                           \
-    OVB_CUDA(cudaFuncSetAttribute(rerank_tc_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    allow_dynamic_smem(rerank_tc_kernel<B>);                                                                    \
     rerank_tc_kernel<B><<<(unsigned)ctas, kRrThreads, smem, stream>>>(map, a);                                  \
   } while (0)
   if (bits == 1)

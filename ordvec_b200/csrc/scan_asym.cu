@@ -314,8 +314,7 @@ void launch_table(uint32_t bits, dim3 grid, size_t smem, cudaStream_t st, const 
                   uint32_t* keys, uint64_t ld) {
 #define OVB_TAB(B)                                                                                     \
   do {                                                                                                 \
-    OVB_CUDA(cudaFuncSetAttribute(asym_table_kernel<B, SUBSET>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                  (int)smem));                                                         \
+    allow_dynamic_smem(asym_table_kernel<B, SUBSET>);                                                  \
     asym_table_kernel<B, SUBSET><<<grid, kTabThreads, smem, st>>>(codes, n, dim, qu, off, cands, inv_norm, \
                                                                   keys, ld);                           \
   } while (0)

@@ -134,8 +134,7 @@ void launch_fastscan_scan(const uint8_t* blocks, uint64_t n, uint32_t pairs_pad,
     const uint8_t* l = lut + q0 * pairs_pad * 16;
 #define OVB_FS(QTV)                                                                                   \
   case QTV:                                                                                           \
-    OVB_CUDA(cudaFuncSetAttribute(fastscan_scan_kernel<QTV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                  (int)smem1));                                                       \
+    allow_dynamic_smem(fastscan_scan_kernel<QTV>);                                                    \
     fastscan_scan_kernel<QTV><<<grid, kThreads, smem1, stream>>>(blocks, n, pairs_pad, l, bias_sum + q0,   \
                                                                  inv_q + q0, inv_norm, rem, keys + q0 * ld, ld); \
     break;

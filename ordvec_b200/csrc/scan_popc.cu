@@ -162,7 +162,7 @@ void launch_rows(int mode, const uint64_t* words, uint64_t n, uint32_t qpv, cons
   // 16-byte loads when every row starts 16-byte aligned
   const bool vec = qpv % 2 == 0 && reinterpret_cast<uintptr_t>(words) % 16 == 0;
   auto kernel = vec ? popc_rows_kernel<QG, true> : popc_rows_kernel<QG, false>;
-  if (smem > 48 * 1024) OVB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(kernel);
   const uint64_t groups = (nq + QG - 1) / QG;
   for (uint64_t g0 = 0; g0 < groups; g0 += 65535) {
     const uint64_t gy = groups - g0 < 65535 ? groups - g0 : 65535;
@@ -210,10 +210,8 @@ void launch_multibucket_scan(const uint64_t* words, uint64_t n, uint32_t qpb, ui
   const size_t smem = (size_t)nb * qpb * 8 + (size_t)nb * nb * 4;
   const bool vec = qpb % 2 == 0 && reinterpret_cast<uintptr_t>(words) % 16 == 0;
   auto kernel = vec ? multibucket_rows_kernel<true> : multibucket_rows_kernel<false>;
-  if (smem > 48 * 1024) {
-    if (smem > 200 * 1024) throw std::invalid_argument("multi-bucket scan: rows too long");
-    OVB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  }
+  if (smem > 200 * 1024) throw std::invalid_argument("multi-bucket scan: rows too long");
+  allow_dynamic_smem(kernel);
   for (uint64_t q0 = 0; q0 < nq; q0 += 65535) {
     unsigned gy = (unsigned)((nq - q0) < 65535 ? (nq - q0) : 65535);
     dim3 grid(scan_grid(kThreads, n), gy);

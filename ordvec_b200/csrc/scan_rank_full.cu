@@ -203,7 +203,7 @@ void launch_tile(const uint16_t* ranks, uint64_t n, uint32_t dim, const void* q,
                  float mean, float scale, uint32_t* keys, uint64_t ld, cudaStream_t stream) {
   const size_t smem = ((size_t)kRfWarps * 32 * kRowWords + (size_t)dim * QT) * 4;
   auto kern = rank_tile_kernel<SYM, QT, WIDE>;
-  if (smem > 48 * 1024) OVB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(kern);
   const uint64_t groups = (nq + QT - 1) / QT;
   uint64_t gy = (n + kRfWarps * 32 - 1) / (kRfWarps * 32);
   // enough CTAs to fill every SM several times over; documents beyond that loop
@@ -254,8 +254,7 @@ void launch_rank_sym_scan(const uint16_t* ranks, uint64_t n, uint32_t dim, const
     return;
   }
   const size_t smem = (size_t)dim * 4;
-  if (smem > 48 * 1024)
-    OVB_CUDA(cudaFuncSetAttribute(rank_sym_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(rank_sym_kernel);
   for (uint64_t q0 = 0; q0 < nq; q0 += 65535) {
     const unsigned gy = (unsigned)(nq - q0 < 65535 ? nq - q0 : 65535);
     rank_sym_kernel<<<dim3(rf_grid(n, kRfThreads / 32), gy), kRfThreads, smem, stream>>>(
@@ -276,8 +275,7 @@ void launch_rank_asym_scan(const uint16_t* ranks, uint64_t n, uint32_t dim, cons
     return;
   }
   const size_t smem = (size_t)dim * 4;
-  if (smem > 48 * 1024)
-    OVB_CUDA(cudaFuncSetAttribute(rank_asym_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(rank_asym_kernel);
   for (uint64_t q0 = 0; q0 < nq; q0 += 65535) {
     const unsigned gy = (unsigned)(nq - q0 < 65535 ? nq - q0 : 65535);
     rank_asym_kernel<<<dim3(rf_grid(n, kRfThreads), gy), kRfThreads, smem, stream>>>(

@@ -490,7 +490,7 @@ static void launch_rank_tc(RtArgs a, uint32_t bits, const void* q_split, uint32_
   dim3 grid((unsigned)(q_tiles * doc_tiles));
 #define OVB_RT(B)                                                                                              \
   do {                                                                                                         \
-    OVB_CUDA(cudaFuncSetAttribute(rank_tc_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    allow_dynamic_smem(rank_tc_kernel<B>);                                                                    \
     rank_tc_kernel<B><<<grid, kRtThreads, smem, stream>>>(map, a);                                            \
   } while (0)
   if (bits == 1)

@@ -691,9 +691,7 @@ void launch_select_rows(const SelectArgs& a, uint64_t rows, uint64_t* scratch,
     const uint64_t bytes = per * (a.ids ? 8 : 4);
     const uint32_t stage = bytes <= kClusterStageBytes ? 1u : 0u;
     const size_t smem = stage ? (size_t)bytes : 0;
-    if (smem > 48 * 1024)
-      OVB_CUDA(cudaFuncSetAttribute(select_rows_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
+    if (smem) allow_dynamic_smem(select_rows_cluster_kernel);  // static 32 KiB + the stage
     select_rows_cluster_kernel<<<(unsigned)(rows * kClusterCtas), kSelThreads, smem, stream>>>(a, stage);
     launched();
     return;

@@ -153,6 +153,7 @@ def test_server_batches_mixed_k_and_m_of_one_route():
     for rq, s1 in _routes()[1:]:
         srv = ob.Server(workers=1, max_batch=1024)
         r = srv.add_route(rq, s1)
+        srv.wait_ready()
         rng = np.random.default_rng(5)
         reqs = []
         for j in range(60):
@@ -160,10 +161,16 @@ def test_server_batches_mixed_k_and_m_of_one_route():
             k = int(rng.choice([10, 50, 100]))
             m = 0 if s1 is None else int(rng.choice([0, 0, 400, 1500]))
             reqs.append((q, k, m))
-        tickets = [srv.submit(r, q, k, m) for q, k, m in reqs]  # all arrive at once
+        # four full-size requests occupy the worker (one batch each) while the
+        # mixed requests queue up behind them
+        big = ob.synth_queries(299, len(rq), 1024, rq.dim)[0]
+        blockers = [srv.submit(r, big, 10, 0) for _ in range(4)]
+        tickets = [srv.submit(r, q, k, m) for q, k, m in reqs]
         got = [t.wait()[0] for t in tickets]
+        for t in blockers:
+            t.wait()
         st = srv.stats()
-        assert st["requests"] == len(reqs) and st["batches"] < len(reqs) // 4
+        assert st["requests"] == len(reqs) + 4 and st["batches"] - 4 < len(reqs) // 4
         for (q, k, m), g in zip(reqs, got):
             want = rq.search_asymmetric(q, k) if s1 is None else ob.two_stage_search(rq, s1, q, m, k)
             assert g.k == want.k
