@@ -805,7 +805,12 @@ def serving_multi_run(ob, seconds: float, rates):
     st = srv.stats()
     out["batches"], out["max_concurrent_batches"] = st["batches"], st["max_concurrent_batches"]
     srv.close()
-    # plain per-request form: one request at a time, host buffers
+    # plain per-request form: one request at a time, host buffers; this thread's
+    # buffers are first sized by one untimed largest request per index (the
+    # server's workers do the same before serving)
+    for j in range(3):
+        for sz in (7, 31, 256):
+            ob.two_stage_search(keep[j][0], keep[j][1], pools[j][:sz], 0, 100)
     rng2 = np.random.default_rng(seed + 1)
     plain_lat, plain_q = [], 0
     for i in range(120):

@@ -168,13 +168,18 @@ void filtered_select(Workspace& w, uint64_t n, uint64_t nq, uint32_t me, const F
 }
 
 // Tensor-core overlap scan for sign bitmaps (Hamming), constant-weight bitmaps
-// and identity-weight multi-bucket bitmaps, batches of at least 32 queries;
+// and identity-weight multi-bucket bitmaps: batches of at least 32 queries, and
+// from 8 queries on indices of at least 2^20 rows whose top-m takes the
+// sampled-threshold filter (the CUDA-core form would write nq key rows of n
+// keys and select m from each: milliseconds at millions of rows, where the
+// filtered scan costs about the same for 8 queries as for 256);
 // OVB_BITMAP_TC=0/1 forces.
-bool use_bitmap_tc(uint64_t nq) {
+bool use_bitmap_tc(uint64_t nq, uint64_t n, uint32_t m) {
   const char* e = getenv("OVB_BITMAP_TC");
   if (e && e[0] == '0') return false;
   if (e && e[0] == '1') return true;
-  return nq >= 32;
+  FilterPlan fp;
+  return nq >= 32 || (nq >= 8 && n >= (1ull << 20) && filter_plan(n, m, fp));
 }
 
 // Stage-1 top-m of a bitmap-family index on the tensor cores: key_kind 0 for a
@@ -562,7 +567,7 @@ uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint6
         launch_bitmap_query(d_q, nq, s1.dim, s1.n_top, qb, st);
       w.mark(st, 1);
       const uint32_t key_bits = bits_for(mode == 0 ? s1.dim : s1.n_top);
-      if (use_bitmap_tc(nq)) {  // sign: Hamming (key kind 2); bitmap: n_top - overlap (0)
+      if (use_bitmap_tc(nq, n, me)) {  // sign: Hamming (key kind 2); bitmap: n_top - overlap (0)
         bitmap_tc_candidates(s1, qb, s1.qpv(), mode == 0 ? 2 : 0, key_bits, nq, me, sk, si, w, st);
         break;
       }
@@ -622,7 +627,7 @@ uint32_t engine_candidates(const Index& s1, const float* d_q, uint64_t nq, uint6
       uint64_t* qb = (uint64_t*)w.qbits.ensure(nq * nb * qpb * 8);
       launch_multibucket_query(d_q, nq, s1.dim, s1.bits, qb, st);
       w.mark(st, 1);
-      if (!d_weights && use_bitmap_tc(nq)) {
+      if (!d_weights && use_bitmap_tc(nq, n, me)) {
         // identity weights: the f32 sum over (a, a) of popcount(Q_a AND D_a)
         // is the integer overlap of the concatenated bucket rows (exact below 2^24)
         bitmap_tc_candidates(s1, qb, nb * qpb, 1, 32, nq, me, sk, si, w, st);

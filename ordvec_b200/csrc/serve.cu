@@ -163,26 +163,39 @@ void run_batch(Server& S, const Route& rt, std::vector<ReqPtr>& batch, uint64_t 
 // Grow this worker's device and pinned buffers to a route's largest batch
 // before it serves requests: buffers only grow, and a growth frees the old
 // allocation, which waits for the whole device and would stall the other
-// workers' batches mid-stream.  Both stage-1 forms are exercised (the <32-query
-// CUDA-core scan with its key rows, and a max_batch tensor-core batch).
+// workers' batches mid-stream.  Both stage-1 forms are exercised (the CUDA-core
+// scan with its key rows below 8 or 32 queries, and tensor-core batches).
+// Two-stage routes also run a ragged batch (requests of different candidate
+// counts: one query at k = 10, the rest at k = 100, the default policy's 320
+// and 3,200 candidates), whose CSR offsets, compacted candidate rows and keys
+// the uniform batches never size.  Requests beyond k = 100 (or explicit m
+// above 3,200) may still grow buffers on first use.
 void warm_route(Server& S, const Route& rt, HostBuf& hq, HostBuf& hs, HostBuf& hi, DevBuf& dq, DevBuf& ds,
                 DevBuf& di) {
   const uint32_t dim = rt.rq->dim;
-  for (uint64_t nq : {(uint64_t)31, (uint64_t)S.max_batch}) {
-    std::vector<ReqPtr> batch(1, std::make_shared<Request>());
-    Request& q = *batch[0];
-    q.nq = nq;
-    q.k = 100;
-    q.m = 0;
-    q.q.resize(nq * dim);
-    uint64_t x = 0x9E3779B97F4A7C15ull;
-    for (float& v : q.q) {  // deterministic, finite, non-degenerate
+  auto make = [&](uint64_t nq, uint64_t k) {
+    auto r = std::make_shared<Request>();
+    r->nq = nq;
+    r->k = k;
+    r->m = 0;
+    r->q.resize(nq * dim);
+    uint64_t x = 0x9E3779B97F4A7C15ull ^ nq;
+    for (float& v : r->q) {  // deterministic, finite, non-degenerate
       x ^= x << 13;
       x ^= x >> 7;
       x ^= x << 17;
       v = (float)((int64_t)(x >> 40) - (1 << 23)) * (1.0f / (1 << 23));
     }
+    return r;
+  };
+  for (uint64_t nq : {(uint64_t)7, (uint64_t)31, (uint64_t)S.max_batch}) {
+    if (nq > S.max_batch) continue;
+    std::vector<ReqPtr> batch(1, make(nq, 100));
     run_batch(S, rt, batch, nq, hq, hs, hi, dq, ds, di);
+    if (rt.s1 && nq >= 2) {
+      std::vector<ReqPtr> ragged{make(1, 10), make(nq - 1, 100)};
+      run_batch(S, rt, ragged, nq, hq, hs, hi, dq, ds, di);
+    }
   }
 }
 
