@@ -295,9 +295,11 @@ ordvec_status_t ovb_two_stage_search_device(const ordvec_index_t *rq,
                                             void *stream);
 /* How the two-stage pipelines rerank (no counterpart in the reference, whose
  * rerank is its asymmetric subset scorer, src/quant.rs:1126-1281):
- *   OVB_RERANK_AUTO       the split-BF16 tensor-core rerank where the shape
- *                         allows it (dim % 64 == 0, 16 <= dim*bits/8 <= 256 and a
- *                         multiple of 16, >= 16 queries, m >= 4k + 64), else FP64
+ *   OVB_RERANK_AUTO       FP64 (the faster form at the measured shapes); with the
+ *                         environment variable OVB_RERANK_TC=1, the split form
+ *                         where the shape allows it (dim % 64 == 0,
+ *                         16 <= dim*bits/8 <= 256 and a multiple of 16, >= 16
+ *                         queries, m >= 4k + 64), else FP64
  *   OVB_RERANK_FP64       every candidate scored in FP64 (per-query tables)
  *   OVB_RERANK_SPLIT      split-BF16 scores (codes exact in BF16, query = hi + lo
  *                         BF16, f32 accumulation on tcgen05), then the top

@@ -590,9 +590,9 @@ RERANK_MODES = {"auto": 0, "fp64": 1, "split": 2, "split_raw": 3}
 def two_stage_search_device(rq: RankQuant, stage1: _Index, d_queries: int, nq: int, m: int, k: int,
                             d_scores: int, d_ids: int, stream: int, rerank: str = "auto") -> None:
     """Device-pointer two-stage search, asynchronous on `stream` (cudaStream_t as int).
-    rerank: "auto" (split-BF16 tensor-core rerank with exact FP64 rescoring where
-    eligible), "fp64", "split" (force the exact split form) or "split_raw" (the
-    split-BF16 scores themselves)."""
+    rerank: "auto" (the FP64 tables, or with OVB_RERANK_TC=1 the split-BF16
+    tensor-core rerank with exact FP64 rescoring where eligible), "fp64", "split"
+    (force the exact split form) or "split_raw" (the split-BF16 scores themselves)."""
     if rerank == "auto":
         check(lib().ovb_two_stage_search_device(rq.handle, stage1.handle, C.c_void_p(d_queries), nq, m, k,
                                                 C.c_void_p(d_scores), C.c_void_p(d_ids), C.c_void_p(stream)))
