@@ -119,7 +119,14 @@ bool filter_plan(uint64_t n, uint32_t m, FilterPlan& p) {
   p.stride = stride;
   p.n_s = n_s;
   p.r = (uint32_t)rr;
-  p.cap = (uint32_t)((8ull * m + 2048 + 31) / 32 * 32);
+  // A query keeps about r * stride docs (relative spread ~ 1 / sqrt(r)); the
+  // capacity covers twice that as well as 8m, since one query over it sends
+  // its whole chunk through the key matrix (with m = 320 at stride 128: r = 24,
+  // ~3,100 kept, and 8m + 2048 alone overflowed for ~0.7 % of queries).
+  const uint64_t by_m = 8ull * m + 2048, by_r = 2ull * p.r * stride + 4096;
+  uint64_t cap = by_m > by_r ? by_m : by_r;
+  if (cap > n + 32) cap = n + 32;
+  p.cap = (uint32_t)((cap + 31) / 32 * 32);
   return true;
 }
 
