@@ -245,6 +245,17 @@ void require_kind(const Index& ix, uint32_t kind, const char* what) {
 
 uint64_t engine_keys_budget() { return keys_budget(); }
 
+uint64_t engine_stage1_bytes(const Index& s1, uint64_t nq, uint64_t m) {
+  const uint64_t n = s1.n;
+  const uint32_t me = (uint32_t)(m < n ? m : n);
+  const bool bitmap = s1.kind == OVB_INDEX_KIND_SIGN_BITMAP || s1.kind == ORDVEC_INDEX_KIND_BITMAP;
+  FilterPlan fp;
+  if (bitmap && me && use_bitmap_tc(nq, n, me) && filter_plan(n, me, fp))
+    return nq * (fp.n_s * 4 + (uint64_t)fp.r * 8 + (uint64_t)fp.cap * 8 + 4);
+  const uint64_t keys = nq * n * 4;
+  return keys < keys_budget() ? keys : keys_budget();
+}
+
 uint64_t default_candidate_count(uint64_t k, uint64_t space) {
   // TwoStageCandidatePolicy::default() (src/quant.rs:242-262): min 256, k*32.
   if (k == 0 || space == 0) return 0;

@@ -185,6 +185,10 @@ uint32_t engine_two_stage_ragged(const Index& rq, const Index& s1, const float* 
                                  const uint64_t* m_of, uint64_t k, Workspace& w, cudaStream_t st);
 uint64_t default_candidate_count(uint64_t k, uint64_t space);
 uint64_t engine_keys_budget();  // bytes a key matrix chunk may take
+// Device bytes of a stage-1 top-m's intermediates for nq queries: the sampled
+// filter's sample keys and kept rows where a bitmap-family stage 1 takes the
+// tensor-core filter, else the key matrix (capped at the chunk budget).
+uint64_t engine_stage1_bytes(const Index& s1, uint64_t nq, uint64_t m);
 // engine_rankquant_split_fixed can run nq queries of top-k in one chunk
 bool split_fixed_fits(const Index& rq, uint64_t nq, uint64_t k);
 

@@ -84,13 +84,13 @@ Server& as_server(ovb_server_t* s) {
   return *p;
 }
 
-// Device bytes a batch needs: query copies, the key rows of its stage-1 /
-// full scan (the engine caps the key matrix at its 2 GiB budget), candidate
-// and result rows.
+// Device bytes a batch needs: query copies, the intermediates of its stage 1
+// (the sampled filter's rows, or a key matrix the engine caps at its 2 GiB
+// budget) or of its full scan, candidate and result rows.
 uint64_t batch_bytes(const Route& r, uint64_t nq, uint64_t k, uint64_t m) {
   const uint64_t n = r.rq->n, dim = r.rq->dim;
   const uint64_t me = r.s1 ? (m ? std::min<uint64_t>(m, n) : default_candidate_count(k, n)) : 0;
-  const uint64_t keys = std::min<uint64_t>(nq * n * 4, 2ull << 30);
+  const uint64_t keys = r.s1 ? engine_stage1_bytes(*r.s1, nq, me) : std::min<uint64_t>(nq * n * 4, 2ull << 30);
   return keys + nq * (12 * dim + 24 * me + 24 * k + 8192);
 }
 
