@@ -107,8 +107,8 @@ bool filter_plan(uint64_t n, uint32_t m, FilterPlan& p) {
   // the doc count, so the sample is kept near 4-8K docs (one wave at <= 256
   // queries); the stride stops at 64, or at 128 from 4M docs (the sample's
   // dense keys and their select take a visible share of a batch there, and
-  // the rank r of the threshold stays in the tens)
-  const uint32_t max_stride = n >= 4000000 ? 128 : 64;
+  // the rank r of the threshold stays in the tens), and at 256 from 8M docs
+  const uint32_t max_stride = n >= 8000000 ? 256 : n >= 4000000 ? 128 : 64;
   while (stride < max_stride && n / (2ull * stride) >= 4096) stride <<= 1;
   const uint64_t n_s = fastscan_tc_sample_docs(n, stride);
   const char* me = getenv("OVB_FASTSCAN_SAMPLE_MULT");
